@@ -1,0 +1,272 @@
+"""Benchmark: plain rips_persistence on n=20000 points in d=10 (H0-H2).
+
+Workload: 20000 i.i.d. N(0,1) float32 points in R^10 from seed 42,
+max_edge_length=1.4, max_dim=2 (the reference's "20K x 10 H0-H2 ms"
+figure). Synthetic data. One step = one full rips_persistence call.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {flashph,reference}]
+
+Prints one JSON line on rank 0. ``value`` is the device-timed ms per call
+with the points resident in HBM; ``e2e`` is the same call made through the
+public API with a pinned host array (host->device copy of the points and
+device->host copy of the diagrams inside the timed region). Under torchrun
+every rank runs an independent replica (the path does not shard); times are
+the max over ranks. ``--impl reference`` times the CPU oracle (a port of the
+reference's algorithm) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "flash-ph_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+N_POINTS, DIM, THRESH, MAX_DIM, SEED = 20000, 10, 1.4, 2, 42
+METRIC = "20Kx10 H0-H2 ms"
+PUBLISHED_MS = 43.0  # reference README.md:103, A100-80GB
+WORKLOAD = ("plain rips_persistence, n=20000 d=10 N(0,1) seed 42, max_edge_length=1.4, "
+            "max_dim=2 (H0-H2), Euclidean, strict filtration")
+
+
+def make_points(seed=SEED):
+    return np.random.default_rng(seed).standard_normal((N_POINTS, DIM)).astype(np.float32)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """CPU oracle (port of the reference algorithm) on all host threads."""
+    if rank != 0:
+        return
+    import oracle
+
+    oracle.build()
+    pts = make_points()
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.run(pts, THRESH, MAX_DIM, fused=True, nthreads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.run(pts, THRESH, MAX_DIM, fused=True, nthreads=cores)
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = statistics.mean(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": round(ms / PUBLISHED_MS, 4),
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": N_POINTS, "d": DIM, "max_edge_length": THRESH,
+                   "max_dim": MAX_DIM},
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "port",
+                         "sample": "the full workload per step (C++ port of the reference algorithm, "
+                                   "edge enumeration on all cores, reduction serial)"},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("flashph", "reference"), default="flashph")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from flashph_b200 import _lib, _timing, rips_persistence
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    pts_np = make_points(SEED + rank)
+    pts = torch.from_numpy(pts_np).to(dev)
+    pinned = torch.from_numpy(pts_np).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def step():
+        return rips_persistence(pts, THRESH, max_dim=MAX_DIM)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    # device-timed region: points resident in HBM, L2 flushed before every step
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    l0 = _lib.launch_count()
+    with ClockSampler(local) as clocks, _timing.record() as stages:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record()
+            out = step()
+            ends[k].record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = (_lib.launch_count() - l0) // args.steps
+    per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = statistics.mean(per)
+    st = _timing.summarize(stages)
+    edge_cnt, edge_ms = st.get("edges", (1, float("nan")))
+    edge_ms /= max(edge_cnt, 1)
+
+    # end to end through the public API with host buffers
+    e2e_ms = []
+    h2d = pinned.numel() * 4
+    d2h = 0
+    for k in range(max(3, args.steps // 2)):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        res = rips_persistence(pinned, THRESH, max_dim=MAX_DIM)  # CPU in, CPU out
+        b.record()
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+        d2h = sum(r.numel() * 4 for r in res)
+    e2e = statistics.mean(e2e_ms)
+
+    vals = torch.tensor([ms, e2e, edge_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms, e2e, edge_ms = (float(x) for x in vals.cpu())
+
+    if rank == 0:
+        pk, src = peaks()
+        cs = clocks.summary()
+        flops = 3.0 * DIM * N_POINTS * (N_POINTS - 1) / 2.0
+        fp32_peak = 148 * 128 * 2 * (pk.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+        achieved = flops / (edge_ms * 1e-3) / 1e12
+        cpu = None
+        if not args.no_cpu_baseline:
+            import oracle
+
+            oracle.build()
+            cores = os.cpu_count() or 1
+            t0 = time.perf_counter()
+            oracle.run(pts_np, THRESH, MAX_DIM, fused=True, nthreads=cores)
+            cpu_ms = (time.perf_counter() - t0) * 1e3
+            cpu = {"value": round(cpu_ms, 2), "unit": "ms", "cores": cores, "kind": "port",
+                   "sample": "one run of the full workload (C++ port of the reference algorithm)"}
+        rows = [int(o.shape[0]) for o in out]
+        line = {
+            "metric": METRIC, "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": round(ms / PUBLISHED_MS, 5), "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N_POINTS, "d": DIM, "max_edge_length": THRESH,
+                       "max_dim": MAX_DIM, "replicas": world,
+                       "l2": "flushed before every timed step (256 MiB write)", "rows": rows},
+            "e2e": {"value": round(e2e, 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": "k_edges (edge enumeration)", "bound": "fp32-alu",
+                         "achieved": round(achieved, 3), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                         "frac": round(achieved / fp32_peak, 4), "traffic": None,
+                         "algorithmic_flops_per_launch": flops, "avg_launch_ms": round(edge_ms, 5),
+                         "peak_source": f"148 SMs x 128 FP32 lanes x 2 x sm_max_mhz ({src} peaks file)"},
+            "cpu_baseline": cpu,
+            "clocks": cs,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,53 @@
+// Shared definitions for the flash-ph B200 CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/flashph_b200.h"
+
+namespace ph {
+
+using i32 = int32_t;
+using i64 = int64_t;
+using u32 = uint32_t;
+using u64 = uint64_t;
+
+constexpr int kWarp = 32;
+
+inline int ceil_div(i64 a, i64 b) { return (int)((a + b - 1) / b); }
+
+// Records the first device-side error code; later codes do not overwrite it.
+__device__ __forceinline__ void set_status(int* status, int code) {
+  if (status) atomicCAS(status, 0, code);
+}
+
+__device__ __forceinline__ u32 lanemask_lt() {
+  u32 m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ u32 float_bits(float f) { return __float_as_uint(f); }
+
+// Remembers the message of a failed CUDA call for ph_last_error().
+void record_error(cudaError_t e);
+
+// Counts kernel launches made by this library (reported by ph_launch_count()).
+void count_launch();
+
+}  // namespace ph
+
+#define PH_CHECK_LAUNCH()                         \
+  do {                                            \
+    cudaError_t _e = cudaGetLastError();          \
+    if (_e != cudaSuccess) {                      \
+      ph::record_error(_e);                       \
+      return PH_ERR_CUDA;                         \
+    }                                             \
+  } while (0)
+
+#define PH_TRY(expr)                  \
+  do {                                \
+    int _rc = (expr);                 \
+    if (_rc != PH_OK) return _rc;     \
+  } while (0)

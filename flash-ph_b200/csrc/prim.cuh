@@ -1,0 +1,41 @@
+// Device-wide primitives written for this library: exclusive scan and a
+// stable LSD radix sort of (u64 key, u32 value) pairs. Both run entirely on
+// the stream with no host synchronisation: the sort decides on the device
+// which 8-bit digits vary and skips the passes of constant digits.
+#pragma once
+#include "common.cuh"
+
+namespace ph {
+
+// ---- exclusive scan -------------------------------------------------------
+// out[0..n] with out[n] = total. In/Out are integer types.
+size_t scan_workspace_bytes(i64 n);
+int scan_exclusive_i32_i32(const i32* in, i32* out, i64 n, void* ws, size_t ws_bytes, cudaStream_t s);
+int scan_exclusive_i32_i64(const i32* in, i64* out, i64 n, void* ws, size_t ws_bytes, cudaStream_t s);
+int scan_exclusive_u8_i32(const uint8_t* in, i32* out, i64 n, void* ws, size_t ws_bytes, cudaStream_t s);
+
+// ---- stable radix sort -----------------------------------------------------
+// Sorts keys[0..n) (and the matching vals) ascending by bits [begin_bit,
+// end_bit) of the key, stably; results end in keys/vals. begin/end multiples of 8.
+size_t radix_sort_workspace_bytes(i64 n);
+int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, void* ws,
+                     size_t ws_bytes, cudaStream_t s);
+
+// Workspace carving helper: aligned bump allocation inside a caller buffer.
+struct Carve {
+  char* base;
+  size_t size;
+  size_t used = 0;
+  Carve(void* p, size_t n) : base(static_cast<char*>(p)), size(n) {}
+  template <typename T>
+  T* take(i64 count) {
+    size_t off = (used + 255) & ~size_t(255);
+    size_t bytes = (size_t)count * sizeof(T);
+    if (off + bytes > size) return nullptr;
+    used = off + bytes;
+    return reinterpret_cast<T*>(base + off);
+  }
+  static size_t need(size_t bytes) { return ((bytes + 255) & ~size_t(255)) + 256; }
+};
+
+}  // namespace ph

@@ -1,0 +1,341 @@
+// Triangles and tetrahedra of the Rips complex, emitted directly in
+// filtration order, and the cofacet (coboundary) CSR built from them.
+//
+// Reference: triangle_kernel.py:28-144,152-270,288-505 (enumeration),
+// reduce_h1_gpu.py:65-152,509-521 (face ranks, triangle order, cofacet CSR).
+//
+// The reference enumerates triangles per edge (third vertex above both
+// endpoints), then looks up face ranks with a sort + searchsorted and orders
+// the triangles with two stable argsorts by (largest edge rank, colex). Here
+// every triangle is generated from its largest edge m = (a, b): its third
+// vertex w is a common neighbour of a and b with both other edges ranked
+// below m. For a fixed largest edge the colex order of {a, b, w} is the order
+// of w, so walking w upward per m yields the reference's (max_rank, colex)
+// order with no sort, and the face ranks fall out of the adjacency walk.
+// Tetrahedra are generated the same way from their largest edge m: pairs
+// p < q of third vertices of m's triangles whose edge (p, q) ranks below m.
+// One warp handles one edge: lanes take 32 consecutive entries of the shorter
+// adjacency row and binary-search the longer one; ballots keep the output in
+// order.
+#include <algorithm>
+
+#include "prim.cuh"
+
+namespace ph {
+namespace {
+
+constexpr int SX_NT = 256;
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int lower_bound_i32(const i32* __restrict__ a, int lo, int hi, i32 x) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// EMIT = false: count; EMIT = true: write triangles.
+template <bool EMIT>
+__global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei, const i32* __restrict__ ej,
+                                                    i64 E, const i32* __restrict__ aptr,
+                                                    const i32* __restrict__ aidx,
+                                                    const i32* __restrict__ arank,
+                                                    i32* __restrict__ tri_cnt, i32* __restrict__ cof_cnt,
+                                                    const i64* __restrict__ tri_off, i32* __restrict__ tm,
+                                                    i32* __restrict__ tw, i32* __restrict__ tfa,
+                                                    i32* __restrict__ tfb) {
+  const int lane = threadIdx.x & 31;
+  const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
+  const u32 lt = lanemask_lt();
+  for (i64 m = warp; m < E; m += nwarps) {
+    const i32 a = ei[m], b = ej[m];
+    int sa = aptr[a], ea = aptr[a + 1], sb = aptr[b], eb = aptr[b + 1];
+    // walk the shorter row, search the longer
+    const bool a_short = (ea - sa) <= (eb - sb);
+    const int s0 = a_short ? sa : sb, s1 = a_short ? ea : eb;
+    const int l0 = a_short ? sb : sa, l1 = a_short ? eb : ea;
+    int ntri = 0, ncof = 0;
+    i64 out = EMIT ? tri_off[m] : 0;
+    for (int base = s0; base < s1; base += 32) {
+      const int p = base + lane;
+      bool common = false, valid = false;
+      i32 w = 0, rs = 0, rl = 0;
+      if (p < s1) {
+        w = aidx[p];
+        rs = arank[p];
+        const int q = lower_bound_i32(aidx, l0, l1, w);
+        if (q < l1 && aidx[q] == w) {
+          common = true;
+          rl = arank[q];
+          valid = rs < (i32)m && rl < (i32)m;
+        }
+      }
+      const u32 cb = __ballot_sync(FULL, common);
+      const u32 vb = __ballot_sync(FULL, valid);
+      if (EMIT && valid) {
+        const i64 o = out + __popc(vb & lt);
+        tm[o] = (i32)m;
+        tw[o] = w;
+        tfa[o] = a_short ? rs : rl;  // rank of (a, w)
+        tfb[o] = a_short ? rl : rs;  // rank of (b, w)
+      }
+      ncof += __popc(cb);
+      ntri += __popc(vb);
+      out += __popc(vb);
+    }
+    if (!EMIT && lane == 0) {
+      tri_cnt[m] = ntri;
+      cof_cnt[m] = ncof;
+    }
+  }
+}
+
+// Tetrahedra with largest edge m: pairs (i < k) of m's triangles whose third
+// vertices p = W[i], q = W[k] are joined by an edge ranked below m.
+template <bool EMIT>
+__global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, const i32* __restrict__ ej, i64 E,
+                                               const i64* __restrict__ tri_off, const i32* __restrict__ tw,
+                                               const i32* __restrict__ tfa, const i32* __restrict__ tfb,
+                                               const i32* __restrict__ aptr, const i32* __restrict__ aidx,
+                                               const i32* __restrict__ arank, i32* __restrict__ tet_cnt,
+                                               const i64* __restrict__ tet_off, i32* __restrict__ qm,
+                                               i32* __restrict__ qf, int* status) {
+  const int lane = threadIdx.x & 31;
+  const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
+  const u32 lt = lanemask_lt();
+  for (i64 m = warp; m < E; m += nwarps) {
+    const i64 t0 = tri_off[m], t1 = tri_off[m + 1];
+    const int nw = (int)(t1 - t0);
+    i64 out = EMIT ? tet_off[m] : 0;
+    int cnt = 0;
+    for (int i = 0; i + 1 < nw; ++i) {
+      const i32 p = tw[t0 + i];
+      const int sp = aptr[p], ep = aptr[p + 1];
+      for (int kb = i + 1; kb < nw; kb += 32) {
+        const int k = kb + lane;
+        bool valid = false;
+        i32 q = 0, rpq = 0;
+        if (k < nw) {
+          q = tw[t0 + k];
+          const int pos = lower_bound_i32(aidx, sp, ep, q);
+          if (pos < ep && aidx[pos] == q) {
+            rpq = arank[pos];
+            valid = rpq < (i32)m;
+          }
+        }
+        const u32 vb = __ballot_sync(FULL, valid);
+        if (EMIT && valid) {
+          const i64 o = out + __popc(vb & lt);
+          qm[o] = (i32)m;
+          qf[4 * o + 0] = (i32)(t0 + i);
+          qf[4 * o + 1] = (i32)(t0 + k);
+          // faces {a, p, q} and {b, p, q}: find their largest edge and third vertex
+          const i32 a = ei[m], b = ej[m];
+#pragma unroll
+          for (int side = 0; side < 2; ++side) {
+            const i32 x = side ? b : a;
+            const i32 rxp = side ? tfb[t0 + i] : tfa[t0 + i];
+            const i32 rxq = side ? tfb[t0 + k] : tfa[t0 + k];
+            i32 M, third;
+            if (rxp > rxq && rxp > rpq) {
+              M = rxp;
+              third = q;
+            } else if (rxq > rpq) {
+              M = rxq;
+              third = p;
+            } else {
+              M = rpq;
+              third = x;
+            }
+            const int lo = (int)tri_off[M], hi = (int)tri_off[M + 1];
+            int f = lower_bound_i32(tw, lo, hi, third);
+            if (f >= hi || tw[f] != third) {  // cannot happen for a consistent adjacency
+              set_status(status, PH_ERR_ARG);
+              f = (int)t0;
+            }
+            qf[4 * o + 2 + side] = f;
+          }
+        }
+        cnt += __popc(vb);
+        out += __popc(vb);
+      }
+    }
+    if (!EMIT && lane == 0) tet_cnt[m] = cnt;
+  }
+}
+
+// Cofacet entries (face, simplex rank) in ascending simplex order.
+__global__ void k_cof_entries(const i32* __restrict__ faos, const i32* __restrict__ f0,
+                              const i32* __restrict__ f1, const i32* __restrict__ f2, int k, i64 S,
+                              i32 row_base, u64* __restrict__ keys, u32* __restrict__ vals) {
+  const i64 total = S * k;
+  for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (i64)gridDim.x * blockDim.x) {
+    const i64 s = x / k;
+    const int z = (int)(x - s * k);
+    i32 f;
+    if (faos) f = faos[x];
+    else f = z == 0 ? f0[s] : (z == 1 ? f1[s] : f2[s]);
+    keys[x] = (u64)(u32)f;
+    vals[x] = (u32)(row_base + s);
+  }
+}
+
+__global__ void k_cof_fill(const u64* __restrict__ keys, const u32* __restrict__ vals, i64 H, i64 nf,
+                           i32* __restrict__ off, i32* __restrict__ data) {
+  for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < H; p += (i64)gridDim.x * blockDim.x) {
+    const i64 f = (i64)keys[p];
+    data[p] = (i32)vals[p];
+    const i64 prev = p ? (i64)keys[p - 1] : -1;
+    for (i64 v = prev + 1; v <= f; ++v) off[v] = (i32)p;
+    if (p == H - 1)
+      for (i64 v = f + 1; v <= nf; ++v) off[v] = (i32)H;
+  }
+}
+
+__global__ void k_cmf(const i32* __restrict__ faos, const i32* __restrict__ f0, const i32* __restrict__ f1,
+                      const i32* __restrict__ f2, int k, i64 S, i32 face_base,
+                      const uint8_t* __restrict__ skip, i32* __restrict__ cmf) {
+  for (i64 s = (i64)blockIdx.x * blockDim.x + threadIdx.x; s < S; s += (i64)gridDim.x * blockDim.x) {
+    i32 best = -1;
+    for (int z = 0; z < k; ++z) {
+      i32 f;
+      if (faos) f = faos[s * k + z];
+      else f = z == 0 ? f0[s] : (z == 1 ? f1[s] : f2[s]);
+      if (!skip[f]) best = max(best, face_base + f);
+    }
+    cmf[s] = best;
+  }
+}
+
+inline int grid_for(i64 n, int nt = 256) {
+  return (int)std::max<i64>(1, std::min<i64>((n + nt - 1) / nt, 148 * 16));
+}
+inline int warp_grid(i64 items) {
+  return (int)std::max<i64>(1, std::min<i64>((items * 32 + SX_NT - 1) / SX_NT, 148 * 32));
+}
+
+}  // namespace
+}  // namespace ph
+
+using namespace ph;
+
+extern "C" size_t ph_triangles_count_workspace_bytes(int64_t E) {
+  return 2 * Carve::need((size_t)(E + 1) * 4) + scan_workspace_bytes(E);
+}
+
+extern "C" int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
+                                  const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                                  int64_t* tri_off, int64_t* cof_off, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (E < 0) return PH_ERR_ARG;
+  Carve c(workspace, workspace_bytes);
+  i32* tc = c.take<i32>(E + 1);
+  i32* cc = c.take<i32>(E + 1);
+  void* sws = c.take<char>((i64)scan_workspace_bytes(E));
+  if (!tc || !cc || !sws) return PH_ERR_ARG;
+  if (E > 0)
+    ph::count_launch();
+    k_triangles<false><<<warp_grid(E), SX_NT, 0, s>>>(edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, tc, cc,
+                                                      nullptr, nullptr, nullptr, nullptr, nullptr);
+  PH_TRY(scan_exclusive_i32_i64(tc, tri_off, E, sws, scan_workspace_bytes(E), s));
+  PH_TRY(scan_exclusive_i32_i64(cc, cof_off, E, sws, scan_workspace_bytes(E), s));
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
+                                 const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                                 const int64_t* tri_off, int32_t* tri_m, int32_t* tri_w, int32_t* tri_fa,
+                                 int32_t* tri_fb, void* stream) {
+  if (E <= 0) return E < 0 ? PH_ERR_ARG : PH_OK;
+  ph::count_launch();
+  k_triangles<true><<<warp_grid(E), SX_NT, 0, (cudaStream_t)stream>>>(
+      edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, nullptr, nullptr, tri_off, tri_m, tri_w, tri_fa, tri_fb);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" size_t ph_tets_count_workspace_bytes(int64_t E) {
+  return Carve::need((size_t)(E + 1) * 4) + scan_workspace_bytes(E);
+}
+
+extern "C" int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64_t E,
+                             const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                             int64_t* tet_off, void* workspace, size_t workspace_bytes, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (E < 0) return PH_ERR_ARG;
+  Carve c(workspace, workspace_bytes);
+  i32* qc = c.take<i32>(E + 1);
+  void* sws = c.take<char>((i64)scan_workspace_bytes(E));
+  if (!qc || !sws) return PH_ERR_ARG;
+  if (E > 0)
+    ph::count_launch();
+    k_tets<false><<<warp_grid(E), SX_NT, 0, s>>>(nullptr, nullptr, E, tri_off, tri_w, nullptr, nullptr, adj_ptr,
+                                                 adj_idx, adj_rank, qc, nullptr, nullptr, nullptr, nullptr);
+  PH_TRY(scan_exclusive_i32_i64(qc, tet_off, E, sws, scan_workspace_bytes(E), s));
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int ph_tets_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int64_t* tri_off,
+                            const int32_t* tri_w, const int32_t* tri_fa, const int32_t* tri_fb,
+                            const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                            const int64_t* tet_off, int32_t* tet_m, int32_t* tet_faces, int* d_status,
+                            void* stream) {
+  if (E <= 0) return E < 0 ? PH_ERR_ARG : PH_OK;
+  ph::count_launch();
+  k_tets<true><<<warp_grid(E), SX_NT, 0, (cudaStream_t)stream>>>(edge_i, edge_j, E, tri_off, tri_w, tri_fa,
+                                                                tri_fb, adj_ptr, adj_idx, adj_rank, nullptr,
+                                                                tet_off, tet_m, tet_faces, d_status);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" size_t ph_cofacet_csr_workspace_bytes(int64_t S, int32_t k) {
+  const i64 H = S * k;
+  return Carve::need((size_t)H * 8) + Carve::need((size_t)H * 4) + radix_sort_workspace_bytes(H);
+}
+
+extern "C" int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const int32_t* f1,
+                              const int32_t* f2, int32_t k, int64_t S, int64_t n_faces, int32_t row_base,
+                              int32_t* cof_off, int32_t* cof_data, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (k < 1 || k > 4 || S < 0 || n_faces < 0) return PH_ERR_ARG;
+  if (!faces_aos && (k != 3 || !f0 || !f1 || !f2)) return PH_ERR_ARG;
+  const i64 H = S * k;
+  if (H >= (int64_t(1) << 31) || (i64)row_base + S >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
+  if (H == 0) {
+    cudaMemsetAsync(cof_off, 0, sizeof(int32_t) * (n_faces + 1), s);
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  Carve c(workspace, workspace_bytes);
+  u64* keys = c.take<u64>(H);
+  u32* vals = c.take<u32>(H);
+  void* rws = c.take<char>((i64)radix_sort_workspace_bytes(H));
+  if (!keys || !vals || !rws) return PH_ERR_ARG;
+  ph::count_launch();
+  k_cof_entries<<<grid_for(H), 256, 0, s>>>(faces_aos, f0, f1, f2, k, S, row_base, keys, vals);
+  PH_TRY(radix_sort_pairs(keys, vals, H, 0, 32, rws, radix_sort_workspace_bytes(H), s));
+  ph::count_launch();
+  k_cof_fill<<<grid_for(H), 256, 0, s>>>(keys, vals, H, n_faces, cof_off, cof_data);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int ph_cof_max_face(const int32_t* faces_aos, const int32_t* f0, const int32_t* f1,
+                               const int32_t* f2, int32_t k, int64_t S, int32_t face_base,
+                               const uint8_t* skip, int32_t* cmf, void* stream) {
+  if (k < 1 || k > 4 || S < 0) return PH_ERR_ARG;
+  if (S == 0) return PH_OK;
+  ph::count_launch();
+  k_cmf<<<grid_for(S), 256, 0, (cudaStream_t)stream>>>(faces_aos, f0, f1, f2, k, S, face_base, skip, cmf);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}

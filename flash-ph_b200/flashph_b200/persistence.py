@@ -1,0 +1,104 @@
+"""Public API: Vietoris-Rips persistent homology (H0, H1, H2) on the B200.
+
+Mirrors ``persistence.py:77-215`` of the reference: the same signature,
+validation messages, edge cases and output convention (a list of
+``max_dim + 1`` float32 ``(K, 2)`` tensors on the input's device, ``inf``
+deaths for essential classes). Every stage runs in the CUDA library; there is
+no CPU path. CPU tensors and numpy arrays are moved to the current CUDA
+device and the results are returned on the input's device.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+from torch import Tensor
+
+from ._lib import check_status
+from .boruvka import boruvka_mask, h0_rows
+from .cohomology import h1_diagram, h2_diagram
+from .rips import edge_filtration_values, rips_filtration
+
+_VERTEX_PACK_BITS = 16
+_VALID_BACKENDS = ("auto", "gpu", "giotto")
+
+
+def _empty(device, k=0):
+    return torch.empty(k, 2, dtype=torch.float32, device=device)
+
+
+def rips_persistence(
+    points,
+    max_edge_length: float,
+    max_dim: int = 1,
+    backend: str = "auto",
+) -> list[Tensor]:
+    """Exact Vietoris-Rips persistent homology (H0 + H1 + optional H2).
+
+    Parameters
+    ----------
+    points : (n, d) array-like
+        Point cloud (numpy arrays are moved to CUDA, as in the reference).
+    max_edge_length : float
+        Edges are kept when dist^2 < fp32(max_edge_length^2) (strict).
+    max_dim : int
+        0, 1 or 2. H2 requires n < 65536.
+    backend : str
+        Accepted for compatibility ('auto', 'gpu', 'giotto'); every value
+        runs the CUDA reduction.
+
+    Returns
+    -------
+    list[Tensor]
+        [H0, H1, ...], each (K, 2) float32 on the input's device.
+    """
+    if isinstance(points, np.ndarray):
+        points = torch.from_numpy(points).float()
+        if torch.cuda.is_available():
+            points = points.cuda()
+    if max_edge_length < 0:
+        raise ValueError(f"max_edge_length must be non-negative, got {max_edge_length}")
+    if points.ndim != 2:
+        raise ValueError(f"points must have shape (n, d), got {tuple(points.shape)}")
+    if max_dim not in (0, 1, 2):
+        raise ValueError(f"max_dim must be 0, 1, or 2, got {max_dim}")
+    if max_dim == 2 and points.shape[0] >= (1 << _VERTEX_PACK_BITS):
+        raise ValueError(
+            f"H2 requires n < {1 << _VERTEX_PACK_BITS} (16-bit vertex packing), "
+            f"got n={points.shape[0]}. Use max_dim=1 or reduce n.")
+    if max_dim == 1 and backend not in _VALID_BACKENDS:
+        raise ValueError(f"backend must be one of {_VALID_BACKENDS}, got {backend!r}")
+
+    out_device = points.device
+    n = points.shape[0]
+    if n == 0:
+        return [_empty(out_device) for _ in range(max_dim + 1)]
+    if n == 1:
+        h0 = torch.tensor([[0.0, float("inf")]], dtype=torch.float32, device=out_device)
+        return [h0] + [_empty(out_device) for _ in range(max_dim)]
+
+    if points.device.type != "cuda":
+        if not torch.cuda.is_available():
+            raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
+        points = points.cuda()
+    dev = points.device
+    with torch.cuda.device(dev):
+        dgms = _compute(points, float(max_edge_length), max_dim)
+    if out_device != dev:
+        dgms = [d.to(out_device) for d in dgms]
+    return dgms
+
+
+def _compute(points: Tensor, t: float, max_dim: int) -> list[Tensor]:
+    n = points.shape[0]
+    filt = rips_filtration(points, t)
+    edge_filt = edge_filtration_values(filt.edge_dist_sq)
+    mst_mask, _, (_, mst_status) = boruvka_mask(filt.edge_i, filt.edge_j, n)
+    h0 = h0_rows(edge_filt, mst_mask, n)
+    if max_dim == 0:
+        check_status("ph_boruvka_mst", mst_status)
+        return [h0]
+    h1, tris, red1, _ = h1_diagram(filt, edge_filt, mst_mask, checks=[("ph_boruvka_mst", mst_status)])
+    if max_dim == 1:
+        return [h0, h1]
+    h2, _, _, _ = h2_diagram(filt, edge_filt, tris, red1)
+    return [h0, h1, h2]

@@ -1,0 +1,230 @@
+/*
+ * flashph_b200.h -- C ABI of the B200 (sm_100a) CUDA library for exact
+ * Vietoris-Rips persistent homology (H0/H1/H2 over Z/2).
+ *
+ * Every entry point takes raw device pointers, element counts and a CUDA
+ * stream (cudaStream_t passed as void*), enqueues its kernels on that stream
+ * and returns a status code without synchronising. Outputs are written into
+ * caller-allocated device buffers; functions that need scratch memory take a
+ * (workspace, workspace_bytes) pair whose size is given by the matching
+ * *_workspace_bytes() query. Counts that the caller needs on the host
+ * (edges, triangles, tetrahedra, diagram rows) are written to device
+ * memory; the caller copies them back when it needs them.
+ *
+ * The functions mirror the internal seams of the reference implementation
+ * (ot-triton-lab/flash-ph, Python); each declaration names the reference
+ * function it replaces. Nothing here calls back into Python, Triton or Numba.
+ */
+#ifndef FLASHPH_B200_H_
+#define FLASHPH_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PH_OK 0
+#define PH_ERR_CUDA 1        /* a CUDA launch or runtime call failed          */
+#define PH_ERR_ARG 2         /* invalid argument or workspace too small      */
+#define PH_ERR_CAPACITY 3    /* an output buffer was too small (count is set) */
+#define PH_ERR_ITER_LIMIT 4  /* a bounded device loop hit its iteration cap  */
+#define PH_ERR_POOL 5        /* reduction column pool exhausted              */
+#define PH_ERR_OVERFLOW 6    /* a count does not fit the index type          */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ph_version(void);
+
+/* Last CUDA error string seen by the library on this thread ("" if none). */
+const char* ph_last_error(void);
+
+/* Number of kernels this library has launched in this process so far. */
+unsigned long long ph_launch_count(void);
+
+/* ---- filtration -------------------------------------------------------- */
+
+/* All pairs i < j with sum_k (x_ik - x_jk)^2 < thr_sq, the squares
+ * accumulated over k = 0..d-1 in order, one fused multiply-add per step,
+ * in FP32. Replaces kernels/edge_kernel.py:152 direct_edge_enumerate (its
+ * count and emit kernels, edge_kernel.py:23-149). Edges are written in an
+ * unspecified order to out_i/out_j/out_dsq up to `capacity`; *d_count (u64,
+ * device) receives the total, which may exceed capacity (then rerun with a
+ * larger buffer). pts: (n, d) float32 row-major. */
+int ph_edges_enumerate(const float* pts, int64_t n, int32_t d, float thr_sq, int32_t* out_i,
+                       int32_t* out_j, float* out_dsq, int64_t capacity,
+                       unsigned long long* d_count, void* stream);
+
+/* Orders E edges by the reference's packed key
+ *   (float bits of dist^2) << 32 | (j(j-1)/2 + i) & 0xFFFFFFFF
+ * stably with respect to the reference kernel's emission order (tiles of 32
+ * points in row-major order, row-major inside a tile), which only matters
+ * when the 32-bit colex part collides (n > 92682). Replaces rips.py:30-50
+ * _pack_sort_key and the stable argsort of rips.py:189-195. Inputs are the
+ * unsorted edges of ph_edges_enumerate; outputs are separate buffers. */
+size_t ph_edges_sort_workspace_bytes(int64_t E);
+int ph_edges_sort(const int32_t* in_i, const int32_t* in_j, const float* in_dsq, int64_t E,
+                  int64_t n, int32_t* out_i, int32_t* out_j, float* out_dsq, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* Per-vertex adjacency with two half-edges per edge, rows sorted by
+ * neighbour index, each entry carrying the edge rank (its position in the
+ * sorted edge list). Replaces rips.py:53-95 _build_vertex_csr.
+ * adj_ptr: n+1, adj_idx/adj_rank: 2E. */
+size_t ph_vertex_csr_workspace_bytes(int64_t E);
+int ph_vertex_csr(const int32_t* edge_i, const int32_t* edge_j, int64_t E, int64_t n,
+                  int32_t* adj_ptr, int32_t* adj_idx, int32_t* adj_rank, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* Square root of each dist^2 (correctly rounded), the edge filtration
+ * values of reduce_h1_gpu.py:479. */
+int ph_sqrt_f32(const float* in, float* out, int64_t count, void* stream);
+
+/* ---- H0 ------------------------------------------------------------------ */
+
+/* Minimum spanning forest under the integer weights edge_rank = position
+ * (ties impossible), as boruvka.py:17 gpu_boruvka_mst computes it. mst_mask[e]
+ * is set to 1 for forest edges; comp[v] receives the smallest vertex index of
+ * v's component (the reference's root labels); *d_ncomp (int64, device) the
+ * number of components. d_status (int, device) gets PH_ERR_ITER_LIMIT if
+ * the bounded round loop does not converge. */
+size_t ph_boruvka_workspace_bytes(int64_t n, int64_t E);
+int ph_boruvka_mst(const int32_t* edge_i, const int32_t* edge_j, int64_t E, int64_t n,
+                   uint8_t* mst_mask, int32_t* comp, int64_t* d_ncomp, int* d_status,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* H0 rows of persistence.py:169-192: (0, sqrt(dist^2)) for the forest edges
+ * in ascending order, then ncomp rows (0, inf); n rows in total.
+ * out_rows: n x 2 float32. */
+size_t ph_h0_rows_workspace_bytes(int64_t E);
+int ph_h0_rows(const float* edge_filt, const uint8_t* mst_mask, int64_t E, int64_t n,
+               float* out_rows, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- triangles (H1 cofacets) -------------------------------------------- */
+
+/* For every edge m = (a, b) (by rank): tri_cnt[m] = number of w with edges
+ * (a,w), (b,w) both ranked below m (the triangles whose largest edge is m),
+ * cof_cnt[m] = number of common neighbours of a and b (the triangles
+ * containing m). Offsets are exclusive scans (E+1 entries, last = total).
+ * Together with ph_triangles_emit this replaces triangle_kernel.py:288
+ * triangle_enumerate and the face-rank lookup and triangle ordering of
+ * reduce_h1_gpu.py:65-100,509-521: triangles come out already ordered by
+ * (largest edge rank, colex), which for a fixed largest edge equals the order
+ * of the third vertex, so the global rank of a triangle is E + its position. */
+size_t ph_triangles_count_workspace_bytes(int64_t E);
+int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
+                       const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                       int64_t* tri_off, int64_t* cof_off, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
+/* Writes, for every triangle in global order, its largest edge tri_m, third
+ * vertex tri_w and the ranks of its two other edges (a,w) and (b,w). */
+int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
+                      const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                      const int64_t* tri_off, int32_t* tri_m, int32_t* tri_w, int32_t* tri_fa,
+                      int32_t* tri_fb, void* stream);
+
+/* ---- tetrahedra (H2 cofacets) ------------------------------------------- */
+
+/* For every edge m: the tetrahedra whose largest edge is m, i.e. pairs
+ * p < q of third vertices of triangles with largest edge m such that (p,q)
+ * is an edge ranked below m. Ordered by (largest edge rank, p, q).
+ * Replaces triangle_kernel.py:402 tetrahedra_enumerate (count and emit
+ * kernels, triangle_kernel.py:152-270). tet_off: E+1. */
+size_t ph_tets_count_workspace_bytes(int64_t E);
+int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64_t E,
+                  const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                  int64_t* tet_off, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Writes per tetrahedron its largest edge and the local indices (triangle
+ * global rank - E) of its four triangle faces. tet_faces: Q x 4.
+ * d_status gets PH_ERR_ARG if a face triangle cannot be found (inconsistent
+ * inputs). */
+int ph_tets_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int64_t* tri_off,
+                 const int32_t* tri_w, const int32_t* tri_fa, const int32_t* tri_fb,
+                 const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
+                 const int64_t* tet_off, int32_t* tet_m, int32_t* tet_faces, int* d_status,
+                 void* stream);
+
+/* ---- coboundary columns and reduction ----------------------------------- */
+
+/* Cofacet CSR: for each of n_faces faces, the global ranks
+ * (row_base + simplex index) of the simplices containing it, ascending.
+ * faces: S x k local face indices of each simplex, simplices given in
+ * ascending order. For triangles (k = 3) the faces are (tri_m, tri_fa,
+ * tri_fb) passed as three separate arrays through faces_soa; for tetrahedra
+ * (k = 4) tet_faces is passed as faces_aos. Replaces reduce_h1_gpu.py:107
+ * _build_cofacet_csr_h1. cof_off: n_faces + 1, cof_data: k*S. */
+size_t ph_cofacet_csr_workspace_bytes(int64_t S, int32_t k);
+int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const int32_t* f1,
+                   const int32_t* f2, int32_t k, int64_t S, int64_t n_faces, int32_t row_base,
+                   int32_t* cof_off, int32_t* cof_data, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/* For every simplex: the largest global rank (face_base + face index) among
+ * its faces that are not skipped, -1 if all are skipped. This is the
+ * cofacet_max_face of reduce_h1_gpu.py:186-197 / cohomology_general.py:50-61. */
+int ph_cof_max_face(const int32_t* faces_aos, const int32_t* f0, const int32_t* f1,
+                    const int32_t* f2, int32_t k, int64_t S, int32_t face_base,
+                    const uint8_t* skip, int32_t* cmf, void* stream);
+
+/* Z/2 cohomology reduction of K columns (faces) over their cofacet rows,
+ * processed in the reference's order (descending rank), pivot = smallest
+ * cofacet rank. Apparent pairs (the column is the largest non-skipped face of
+ * its youngest cofacet) are detected first (reduce_h1_gpu.py:159-223); the
+ * remaining columns are reduced on the GPU by rounds in which every column
+ * whose pivot is claimed by an earlier-processed column adds that column.
+ * The pivots, and so the pairs and the essential columns, are those of the
+ * serial reduction (cohomology_general.py:202-371).
+ * col_state[c]: 0 skipped, 1 apparent, 2 reduced to a pivot, 3 essential.
+ * col_piv[c]: pivot global rank (states 1 and 2) or -1.
+ * pool: scratch for reduced columns, pool_cap int32 entries.
+ * d_info (int64 x 4, device): [residual columns, rounds, pool entries used, 0].
+ * d_status: PH_ERR_POOL or PH_ERR_ITER_LIMIT on failure. */
+size_t ph_reduce_workspace_bytes(int64_t K, int64_t R);
+int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,
+              int64_t R, int32_t row_base, const uint8_t* skip, const int32_t* row_cmf,
+              int32_t* col_state, int32_t* col_piv, int32_t* pool, int64_t pool_cap,
+              int64_t* d_info, int* d_status, void* workspace, size_t workspace_bytes,
+              void* stream);
+
+/* Marks the rows that are pivots of reduced or apparent columns (the H1
+ * pivots that clear H2 columns, cohomology_general.py:171-173,635). */
+int ph_mark_pivots(const int32_t* col_state, const int32_t* col_piv, int64_t K, int32_t row_base,
+                   uint8_t* row_flag, int64_t R, void* stream);
+
+/* Persistence rows in the reference's order (reduce_h1_gpu.py:574-604):
+ * apparent pairs by ascending column, then reduced pairs and essential
+ * columns by descending column, pairs kept when death > birth (as float32),
+ * then a stable sort by birth. Column c's value is filt[col_m ? col_m[c] : c],
+ * row r's value is filt[row_m[r]]. out_rows: capacity K x 2; *d_nrows (int64). */
+size_t ph_persistence_rows_workspace_bytes(int64_t K);
+int ph_persistence_rows(const int32_t* col_state, const int32_t* col_piv, int64_t K,
+                        int32_t row_base, const float* filt, const int32_t* col_m,
+                        const int32_t* row_m, float* out_rows, int64_t* d_nrows, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* ---- thresholds ---------------------------------------------------------- */
+
+/* k-th nearest-neighbour Euclidean distance of every point (self excluded),
+ * threshold.py:133-176 _tiled_knn. k <= 64. out: n float32. */
+int ph_knn_kth(const float* pts, int64_t n, int32_t d, int32_t k, float* out, void* stream);
+
+/* Linear-interpolation quantile of n values (torch.quantile semantics, as
+ * threshold.py:77 uses it); *d_out (float32, device). */
+size_t ph_quantile_workspace_bytes(int64_t n);
+int ph_quantile_f32(const float* values, int64_t n, double q, float* d_out, void* workspace,
+                    size_t workspace_bytes, void* stream);
+
+/* min over points of the max distance to any point, threshold.py:179-200
+ * _tiled_enclosing_radius; *d_out (float32, device). */
+size_t ph_enclosing_radius_workspace_bytes(int64_t n);
+int ph_enclosing_radius(const float* pts, int64_t n, int32_t d, float* d_out, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLASHPH_B200_H_ */

@@ -1,0 +1,106 @@
+"""Python handle on the CPU oracle (test infrastructure only).
+
+The oracle (``ph_oracle.cpp``) restates the reference implementation's
+algorithm on the CPU. Only the tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` use it, always as the checker or as the
+timed CPU baseline, never as part of the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libph_oracle.so")
+
+_lib = None
+_DT = {1: np.int32, 2: np.int64, 3: np.float32}
+ARRAYS = ("edge_i", "edge_j", "edge_dsq", "mst_idx", "h0", "tri_max_rank_sorted",
+          "ap_births", "ap_deaths", "res_births", "res_deaths", "ess_births",
+          "h1_all_pivots", "h1", "h2", "h2_births", "h2_deaths", "h2_ess")
+SCALARS = ("E", "n_components", "T", "Q", "cofacet_nnz", "n_apparent", "residual")
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with make (a no-op when it is up to date)."""
+    if force or not os.path.exists(LIB_PATH) or (
+            os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "ph_oracle.cpp"))):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.oracle_run.restype = ctypes.c_void_p
+        lib.oracle_run.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                   ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                   ctypes.c_int64]
+        lib.oracle_error.restype = ctypes.c_char_p
+        lib.oracle_error.argtypes = [ctypes.c_void_p]
+        lib.oracle_free.argtypes = [ctypes.c_void_p]
+        lib.oracle_get.restype = ctypes.c_void_p
+        lib.oracle_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
+        lib.oracle_scalar.restype = ctypes.c_int64
+        lib.oracle_scalar.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+        lib.oracle_threshold_sq.restype = ctypes.c_float
+        lib.oracle_threshold_sq.argtypes = [ctypes.c_double]
+        _lib = lib
+    return _lib
+
+
+def threshold_sq(max_edge_length: float) -> np.float32:
+    return np.float32(_load().oracle_threshold_sq(float(max_edge_length)))
+
+
+def run(points, max_edge_length: float, max_dim: int = 1, fused: bool = True,
+        nthreads: int = 0, stop_after: int = 0, edge_filt=None) -> dict:
+    """Run the oracle pipeline; returns a dict of numpy arrays and ints.
+
+    ``fused=True`` accumulates dist^2 with a fused multiply-add per
+    dimension (the compiled GPU kernel's arithmetic); ``fused=False`` uses a
+    separate multiply and add (the reference kernel under the Triton
+    interpreter). ``stop_after``: 0 everything, 1 filtration only, 2 through H0.
+    ``edge_filt``: optional filtration value per sorted edge, used instead of
+    the correctly rounded square root of dist^2.
+    """
+    lib = _load()
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+    if pts.ndim != 2:
+        raise ValueError("points must be (n, d)")
+    n, d = pts.shape
+    ov = None if edge_filt is None else np.ascontiguousarray(edge_filt, dtype=np.float32)
+    h = lib.oracle_run(pts.ctypes.data if n else None, n, d, float(max_edge_length),
+                       int(max_dim), int(bool(fused)), int(nthreads), int(stop_after),
+                       None if ov is None or ov.size == 0 else ov.ctypes.data,
+                       -1 if ov is None else ov.size)
+    try:
+        err = lib.oracle_error(h)
+        if err:
+            raise ValueError(err.decode())
+        out = {}
+        for name in ARRAYS:
+            cnt = ctypes.c_int64()
+            dt = ctypes.c_int()
+            ptr = lib.oracle_get(h, name.encode(), ctypes.byref(cnt), ctypes.byref(dt))
+            dtype = _DT[dt.value]
+            if cnt.value > 0:
+                buf = (ctypes.c_char * (cnt.value * np.dtype(dtype).itemsize)).from_address(ptr)
+                arr = np.frombuffer(buf, dtype=dtype).copy()
+            else:
+                arr = np.zeros(0, dtype=dtype)
+            if name in ("h0", "h1", "h2"):
+                arr = arr.reshape(-1, 2)
+            out[name] = arr
+        for name in SCALARS:
+            out[name] = int(lib.oracle_scalar(h, name.encode()))
+    finally:
+        lib.oracle_free(h)
+    return out

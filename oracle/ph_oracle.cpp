@@ -1,0 +1,688 @@
+// CPU oracle for exact Vietoris-Rips persistent homology (H0/H1/H2 over Z/2).
+//
+// TEST INFRASTRUCTURE ONLY. This file restates, step by step, the algorithm
+// of the reference implementation (ot-triton-lab/flash-ph) so that the CUDA
+// path can be checked against it. It is never the thing measured or shipped:
+// only the tests, the smoke check and the CPU-baseline leg of bench.py load
+// it. Every function cites the reference file:line it follows.
+//
+// Build: make -C oracle   (produces oracle/_build/libph_oracle.so)
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <unordered_map>
+#include <vector>
+#include <atomic>
+#include <thread>
+
+namespace {
+
+using i32 = int32_t;
+using i64 = int64_t;
+using u32 = uint32_t;
+using u64 = uint64_t;
+
+struct Result {
+  // sorted filtration (rips.py:15-27)
+  std::vector<i32> edge_i, edge_j;
+  std::vector<float> edge_dsq;
+  // H0 (boruvka.py, persistence.py:169-192)
+  std::vector<i64> mst_idx;
+  i64 n_components = 0;
+  std::vector<float> h0;
+  // H1 (reduce_h1_gpu.py:438-604)
+  i64 T = 0, cofacet_nnz = 0, n_apparent = 0, residual = 0;
+  std::vector<i32> tri_max_rank_sorted;
+  std::vector<i32> ap_births, ap_deaths, res_births, res_deaths, ess_births;
+  std::vector<i32> h1_all_pivots;
+  std::vector<float> h1;
+  // H2 (assembled from triangle_kernel.py:402, cohomology_general.py:32)
+  i64 Q = 0;
+  std::vector<float> h2;
+  std::vector<i32> h2_births, h2_deaths, h2_ess;
+  std::string error;
+};
+
+inline u32 fbits(float f) {
+  u32 u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+// --- edge enumeration: kernels/edge_kernel.py:23-149,152-224 -------------
+// Tiles of B=32 points, programs (I, J) with I <= J in row-major order of the
+// flattened nb x nb grid (prefix at edge_kernel.py:208-210); inside a tile the
+// emitted order is row-major over (source offset, target offset)
+// (edge_kernel.py:134-149). dist^2 is accumulated over k = 0..d-1 in order
+// (edge_kernel.py:111-123): fused (one rounding per step, fmaf) or as a
+// separate multiply and add (this file is compiled with -ffp-contract=off).
+template <bool FUSED>
+static void tile_row(const float* pts, i64 n, int d, float thr_sq, i64 I, i64 nb,
+                     std::vector<i32>& vi, std::vector<i32>& vj, std::vector<float>& vd) {
+  const i64 B = 32;
+  for (i64 J = I; J < nb; ++J) {
+    for (i64 a = 0; a < B; ++a) {
+      const i64 i = I * B + a;
+      if (i >= n) break;
+      const float* x = pts + i * d;
+      for (i64 b = (I == J ? a + 1 : 0); b < B; ++b) {
+        const i64 j = J * B + b;
+        if (j >= n) break;
+        const float* y = pts + j * d;
+        float acc = 0.0f;
+        for (int k = 0; k < d; ++k) {
+          const float df = x[k] - y[k];
+          if (FUSED) acc = __builtin_fmaf(df, df, acc);
+          else acc = acc + df * df;
+        }
+        if (acc < thr_sq) {
+          vi.push_back((i32)i);
+          vj.push_back((i32)j);
+          vd.push_back(acc);
+        }
+      }
+    }
+  }
+}
+__attribute__((target("fma"))) static void tile_row_fma_hw(
+    const float* pts, i64 n, int d, float thr_sq, i64 I, i64 nb,
+    std::vector<i32>& vi, std::vector<i32>& vj, std::vector<float>& vd) {
+  tile_row<true>(pts, n, d, thr_sq, I, nb, vi, vj, vd);
+}
+
+void enumerate_edges(const float* pts, i64 n, int d, float thr_sq, int fused,
+                     int nthreads, std::vector<i32>& oi, std::vector<i32>& oj,
+                     std::vector<float>& odsq) {
+  const i64 B = 32;
+  const i64 nb = (n + B - 1) / B;
+  const bool hw_fma = __builtin_cpu_supports("fma");
+  std::vector<std::vector<i32>> ri(nb), rj(nb);
+  std::vector<std::vector<float>> rd(nb);
+  // Tile rows are independent; threads take them dynamically (largest rows
+  // first) and the per-row lists are concatenated in row order afterwards, so
+  // the emitted order does not depend on the thread count.
+  std::atomic<i64> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const i64 I = next.fetch_add(1);
+      if (I >= nb) break;
+      if (!fused) tile_row<false>(pts, n, d, thr_sq, I, nb, ri[I], rj[I], rd[I]);
+      else if (hw_fma) tile_row_fma_hw(pts, n, d, thr_sq, I, nb, ri[I], rj[I], rd[I]);
+      else tile_row<true>(pts, n, d, thr_sq, I, nb, ri[I], rj[I], rd[I]);
+    }
+  };
+  int nt = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
+  if (nt > nb) nt = (int)std::max<i64>(1, nb);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
+  for (i64 I = 0; I < nb; ++I) {
+    oi.insert(oi.end(), ri[I].begin(), ri[I].end());
+    oj.insert(oj.end(), rj[I].begin(), rj[I].end());
+    odsq.insert(odsq.end(), rd[I].begin(), rd[I].end());
+  }
+}
+
+// --- filtration sort: rips.py:30-50,188-202 --------------------------------
+// key = (float bits of dist^2) << 32 | (j(j-1)/2 + i) & 0xFFFFFFFF, stable.
+void sort_edges(std::vector<i32>& ei, std::vector<i32>& ej, std::vector<float>& ed) {
+  const size_t E = ei.size();
+  std::vector<u64> key(E);
+  for (size_t e = 0; e < E; ++e) {
+    u64 j = (u64)ej[e], i = (u64)ei[e];
+    u64 colex = j * (j - 1) / 2 + i;
+    key[e] = ((u64)fbits(ed[e]) << 32) | (colex & 0xFFFFFFFFull);
+  }
+  std::vector<i64> perm(E);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](i64 a, i64 b) { return key[a] < key[b]; });
+  std::vector<i32> a(E), b(E);
+  std::vector<float> c(E);
+  for (size_t k = 0; k < E; ++k) {
+    a[k] = ei[perm[k]];
+    b[k] = ej[perm[k]];
+    c[k] = ed[perm[k]];
+  }
+  ei.swap(a);
+  ej.swap(b);
+  ed.swap(c);
+}
+
+// --- vertex CSR: rips.py:53-95 (rows sorted by neighbour index) -----------
+struct CSR {
+  std::vector<i32> ptr, idx, rank;
+};
+CSR vertex_csr(const std::vector<i32>& ei, const std::vector<i32>& ej, i64 n) {
+  CSR g;
+  const i64 E = (i64)ei.size();
+  g.ptr.assign(n + 1, 0);
+  for (i64 e = 0; e < E; ++e) {
+    g.ptr[ei[e] + 1]++;
+    g.ptr[ej[e] + 1]++;
+  }
+  for (i64 v = 0; v < n; ++v) g.ptr[v + 1] += g.ptr[v];
+  g.idx.resize(2 * E);
+  g.rank.resize(2 * E);
+  std::vector<i32> fill(g.ptr.begin(), g.ptr.end() - 1);
+  for (i64 e = 0; e < E; ++e) {
+    int p = fill[ei[e]]++;
+    g.idx[p] = ej[e];
+    g.rank[p] = (i32)e;
+    p = fill[ej[e]]++;
+    g.idx[p] = ei[e];
+    g.rank[p] = (i32)e;
+  }
+  std::vector<std::pair<i32, i32>> tmp;
+  for (i64 v = 0; v < n; ++v) {
+    tmp.clear();
+    for (int p = g.ptr[v]; p < g.ptr[v + 1]; ++p) tmp.emplace_back(g.idx[p], g.rank[p]);
+    std::sort(tmp.begin(), tmp.end());
+    for (size_t k = 0; k < tmp.size(); ++k) {
+      g.idx[g.ptr[v] + k] = tmp[k].first;
+      g.rank[g.ptr[v] + k] = tmp[k].second;
+    }
+  }
+  return g;
+}
+
+// --- Boruvka: boruvka.py:17-113, round for round ---------------------------
+void boruvka(const std::vector<i32>& ei, const std::vector<i32>& ej, i64 n,
+             std::vector<i64>& mst, i64& ncomp) {
+  const i64 E = (i64)ei.size();
+  std::vector<i64> comp(n);
+  std::iota(comp.begin(), comp.end(), 0);
+  std::vector<char> in_mst(E, 0);
+  auto flatten = [&]() {
+    std::vector<i64> nc(n);
+    for (int it = 0; it < 64; ++it) {
+      bool same = true;
+      for (i64 v = 0; v < n; ++v) {
+        nc[v] = comp[comp[v]];
+        if (nc[v] != comp[v]) same = false;
+      }
+      if (same) break;
+      comp.swap(nc);
+    }
+  };
+  const int max_iters = (int)std::ceil(std::log2((double)std::max<i64>(n, 2))) + 2;
+  const i64 SENT = INT64_MAX;
+  std::vector<i64> min_key(n);
+  std::vector<char> seen(n);
+  for (int r = 0; r < max_iters; ++r) {
+    flatten();
+    std::fill(seen.begin(), seen.end(), 0);
+    i64 K = 0;
+    for (i64 v = 0; v < n; ++v)
+      if (!seen[comp[v]]) {
+        seen[comp[v]] = 1;
+        ++K;
+      }
+    if (K == 1) break;
+    std::fill(min_key.begin(), min_key.end(), SENT);
+    bool any = false;
+    for (i64 e = 0; e < E; ++e) {
+      i64 cu = comp[ei[e]], cv = comp[ej[e]];
+      if (cu == cv) continue;
+      any = true;
+      min_key[cu] = std::min(min_key[cu], e);
+      min_key[cv] = std::min(min_key[cv], e);
+    }
+    if (!any) break;
+    std::vector<i64> sel;
+    for (i64 c = 0; c < n; ++c)
+      if (min_key[c] < SENT) sel.push_back(min_key[c]);
+    std::sort(sel.begin(), sel.end());
+    sel.erase(std::unique(sel.begin(), sel.end()), sel.end());
+    std::vector<std::pair<i64, i64>> hooks;
+    for (i64 e : sel) {
+      in_mst[e] = 1;
+      i64 su = comp[ei[e]], sv = comp[ej[e]];
+      hooks.emplace_back(std::max(su, sv), std::min(su, sv));
+    }
+    for (auto& h : hooks) comp[h.first] = std::min(comp[h.first], h.second);
+  }
+  flatten();
+  mst.clear();
+  for (i64 e = 0; e < E; ++e)
+    if (in_mst[e]) mst.push_back(e);
+  std::vector<char> s2(n, 0);
+  ncomp = 0;
+  for (i64 v = 0; v < n; ++v)
+    if (!s2[comp[v]]) {
+      s2[comp[v]] = 1;
+      ++ncomp;
+    }
+}
+
+// --- Z/2 column store used by the reducers (cohomology_general.py) ---------
+// The reference keeps reduced columns in a pool addressed through an
+// open-addressing hash map keyed by pivot (_numba_utils.py:14-40); a map from
+// pivot to column is the same mapping.
+using Col = std::vector<i32>;
+void xor_into(Col& cur, const Col& other, Col& tmp) {  // _numba_utils.py:43-65
+  tmp.clear();
+  size_t a = 0, b = 0;
+  while (a < cur.size() && b < other.size()) {
+    if (cur[a] < other[b]) tmp.push_back(cur[a++]);
+    else if (cur[a] > other[b]) tmp.push_back(other[b++]);
+    else { ++a; ++b; }
+  }
+  while (a < cur.size()) tmp.push_back(cur[a++]);
+  while (b < other.size()) tmp.push_back(other[b++]);
+  cur.swap(tmp);
+}
+
+// Sorted-vertex colex ids (cohomology_general.py:378-415, overflow-safe tet
+// form apparent_pair_h2_kernel.py:53-58).
+inline i64 tri_colex(i64 a, i64 b, i64 c) { return c * (c - 1) * (c - 2) / 6 + b * (b - 1) / 2 + a; }
+inline i64 tet_colex(i64 a, i64 b, i64 c, i64 d) {
+  i64 hi = d * (d - 1) / 2, lo = (d - 2) * (d - 3) / 2;
+  return hi * lo / 6 + c * (c - 1) * (c - 2) / 6 + b * (b - 1) / 2 + a;
+}
+
+i32 edge_rank_lookup(const CSR& g, i32 s, i32 t) {  // apparent_pair_h2_kernel.py:37-49
+  int lo = g.ptr[s], hi = g.ptr[s + 1];
+  while (lo < hi) {
+    int mid = (lo + hi) / 2;
+    if (g.idx[mid] < t) lo = mid + 1;
+    else if (g.idx[mid] > t) hi = mid;
+    else return g.rank[mid];
+  }
+  return -1;
+}
+
+void stable_sort_rows_by_birth(std::vector<float>& rows) {
+  const size_t K = rows.size() / 2;
+  std::vector<size_t> p(K);
+  std::iota(p.begin(), p.end(), 0);
+  std::stable_sort(p.begin(), p.end(), [&](size_t a, size_t b) { return rows[2 * a] < rows[2 * b]; });
+  std::vector<float> out(rows.size());
+  for (size_t k = 0; k < K; ++k) {
+    out[2 * k] = rows[2 * p[k]];
+    out[2 * k + 1] = rows[2 * p[k] + 1];
+  }
+  rows.swap(out);
+}
+
+struct Triangles {  // triangle_kernel.py:288-399 output, plus ranks
+  std::vector<i32> v0, v1, v2, mr;
+  std::vector<i32> grank;      // global rank E + position in (max_rank, colex) order
+  std::vector<i32> sorted_idx; // triangle index at each sorted position
+};
+
+// triangle_kernel.py:81-144 / _numba_utils.py:111-183: per edge in rank order,
+// common neighbours w > v in increasing order; max_rank over the three edges.
+Triangles enumerate_triangles(const std::vector<i32>& ei, const std::vector<i32>& ej, const CSR& g) {
+  Triangles t;
+  const i64 E = (i64)ei.size();
+  for (i64 e = 0; e < E; ++e) {
+    i32 u = std::min(ei[e], ej[e]), v = std::max(ei[e], ej[e]);
+    int iu = g.ptr[u], iv = g.ptr[v];
+    const int ue = g.ptr[u + 1], ve = g.ptr[v + 1];
+    while (iu < ue && iv < ve) {
+      i32 nu = g.idx[iu], nv = g.idx[iv];
+      if (nu == nv) {
+        if (nu > v) {
+          t.v0.push_back(u);
+          t.v1.push_back(v);
+          t.v2.push_back(nu);
+          t.mr.push_back(std::max<i32>((i32)e, std::max(g.rank[iu], g.rank[iv])));
+        }
+        ++iu;
+        ++iv;
+      } else if (nu < nv) {
+        ++iu;
+      } else {
+        ++iv;
+      }
+    }
+  }
+  // reduce_h1_gpu.py:509-521: order by (max_rank, colex), global rank = E + pos
+  const i64 T = (i64)t.v0.size();
+  std::vector<i64> colex(T);
+  for (i64 k = 0; k < T; ++k) colex[k] = tri_colex(t.v0[k], t.v1[k], t.v2[k]);
+  t.sorted_idx.resize(T);
+  std::iota(t.sorted_idx.begin(), t.sorted_idx.end(), 0);
+  std::stable_sort(t.sorted_idx.begin(), t.sorted_idx.end(),
+                   [&](i32 a, i32 b) { return colex[a] < colex[b]; });
+  std::stable_sort(t.sorted_idx.begin(), t.sorted_idx.end(),
+                   [&](i32 a, i32 b) { return t.mr[a] < t.mr[b]; });
+  t.grank.resize(T);
+  for (i64 p = 0; p < T; ++p) t.grank[t.sorted_idx[p]] = (i32)(E + p);
+  return t;
+}
+
+// reduce_h1_gpu.py:438-604 (apparent pairs reduce_h1_gpu.py:159-223, residual
+// reduction cohomology_general.py:202-371 with the pool prepopulated by the
+// apparent columns, _numba_utils.py:68-104).
+void h1_native(Result& R, i64 n, const CSR& g, const Triangles& tr, const std::vector<char>& mst_mask,
+               const std::vector<float>& edge_filt) {
+  const i64 E = (i64)R.edge_i.size();
+  const i64 T = (i64)tr.v0.size();
+  R.T = T;
+  if (T == 0) {  // reduce_h1_gpu.py:495-502
+    for (i64 e = 0; e < E; ++e)
+      if (!mst_mask[e]) {
+        R.h1.push_back(edge_filt[e]);
+        R.h1.push_back(INFINITY);
+      }
+    stable_sort_rows_by_birth(R.h1);
+    return;
+  }
+  // face ranks (reduce_h1_gpu.py:65-100) and cofacet CSR (:107-152)
+  std::vector<std::vector<i32>> cof(E);
+  for (i64 k = 0; k < T; ++k) {
+    i32 a = tr.v0[k], b = tr.v1[k], c = tr.v2[k];
+    i32 f[3] = {edge_rank_lookup(g, a, b), edge_rank_lookup(g, a, c), edge_rank_lookup(g, b, c)};
+    for (int q = 0; q < 3; ++q) cof[f[q]].push_back(tr.grank[k]);
+  }
+  for (auto& r : cof) std::sort(r.begin(), r.end());
+  for (auto& r : cof) R.cofacet_nnz += (i64)r.size();
+  // rank_to_filt (reduce_h1_gpu.py:528-530)
+  std::vector<float> r2f(edge_filt);
+  for (i64 p = 0; p < T; ++p) r2f.push_back(edge_filt[tr.mr[tr.sorted_idx[p]]]);
+  R.tri_max_rank_sorted.resize(T);
+  for (i64 p = 0; p < T; ++p) R.tri_max_rank_sorted[p] = tr.mr[tr.sorted_idx[p]];
+  // cof_max_face: max non-skipped face rank of each cofacet
+  std::vector<i32> cmf(E + T, -1);
+  for (i64 e = 0; e < E; ++e) {
+    if (mst_mask[e]) continue;
+    for (i32 t : cof[e]) cmf[t] = std::max(cmf[t], (i32)e);
+  }
+  std::vector<char> is_app(E, 0);
+  std::map<i32, Col> table;
+  for (i64 e = 0; e < E; ++e) {
+    if (cof[e].empty() || mst_mask[e]) continue;
+    if (cmf[cof[e][0]] == (i32)e) {
+      is_app[e] = 1;
+      R.n_apparent++;
+      i32 piv = cof[e][0];
+      R.h1_all_pivots.push_back(piv);
+      if (r2f[piv] > r2f[e]) {
+        R.ap_births.push_back((i32)e);
+        R.ap_deaths.push_back(piv);
+      }
+      table[piv] = cof[e];
+    }
+  }
+  Col cur, tmp;
+  for (i64 e = E - 1; e >= 0; --e) {
+    if (mst_mask[e] || is_app[e]) continue;
+    R.residual++;
+    if (cof[e].empty()) {
+      R.ess_births.push_back((i32)e);
+      continue;
+    }
+    cur = cof[e];
+    while (!cur.empty()) {
+      auto it = table.find(cur[0]);
+      if (it == table.end()) break;
+      xor_into(cur, it->second, tmp);
+    }
+    if (!cur.empty()) {
+      i32 piv = cur[0];
+      R.h1_all_pivots.push_back(piv);
+      table[piv] = cur;
+      if (r2f[piv] > r2f[e]) {
+        R.res_births.push_back((i32)e);
+        R.res_deaths.push_back(piv);
+      }
+    } else {
+      R.ess_births.push_back((i32)e);
+    }
+  }
+  // assembly (reduce_h1_gpu.py:574-604)
+  for (size_t k = 0; k < R.ap_births.size(); ++k) {
+    R.h1.push_back(r2f[R.ap_births[k]]);
+    R.h1.push_back(r2f[R.ap_deaths[k]]);
+  }
+  for (size_t k = 0; k < R.res_births.size(); ++k) {
+    R.h1.push_back(r2f[R.res_births[k]]);
+    R.h1.push_back(r2f[R.res_deaths[k]]);
+  }
+  for (i32 e : R.ess_births) {
+    R.h1.push_back(r2f[e]);
+    R.h1.push_back(INFINITY);
+  }
+  stable_sort_rows_by_birth(R.h1);
+}
+
+// H2: tetrahedra (triangle_kernel.py:152-270 / _numba_utils.py:186-284),
+// ordered by (max_rank, colex) (apparent_pair_h2_kernel.py:117-121), columns
+// are the triangles in their global order with the H1 pivots cleared, reduced
+// by the general cohomology reducer (cohomology_general.py:32-199).
+void h2_blocks(Result& R, const CSR& g, const Triangles& tr, const std::vector<float>& edge_filt) {
+  const i64 E = (i64)R.edge_i.size();
+  const i64 T = (i64)tr.v0.size();
+  std::vector<i32> q0, q1, q2, q3, qmr;
+  for (i64 k = 0; k < T; ++k) {
+    i32 a = tr.v0[k], b = tr.v1[k], c = tr.v2[k];
+    int ia = g.ptr[a], ib = g.ptr[b], ic = g.ptr[c];
+    const int ae = g.ptr[a + 1], be = g.ptr[b + 1], ce = g.ptr[c + 1];
+    while (ia < ae && ib < be && ic < ce) {
+      i32 na = g.idx[ia], nb = g.idx[ib], nc = g.idx[ic];
+      i32 mx = std::max(na, std::max(nb, nc));
+      if (na == nb && nb == nc) {
+        if (na > c) {
+          q0.push_back(a);
+          q1.push_back(b);
+          q2.push_back(c);
+          q3.push_back(na);
+          qmr.push_back(std::max(tr.mr[k], std::max(g.rank[ia], std::max(g.rank[ib], g.rank[ic]))));
+        }
+        ++ia;
+        ++ib;
+        ++ic;
+      } else {
+        if (na < mx) ++ia;
+        if (nb < mx) ++ib;
+        if (nc < mx) ++ic;
+      }
+    }
+  }
+  const i64 Q = (i64)q0.size();
+  R.Q = Q;
+  std::vector<i64> colex(Q);
+  for (i64 k = 0; k < Q; ++k) colex[k] = tet_colex(q0[k], q1[k], q2[k], q3[k]);
+  std::vector<i32> ord(Q);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](i32 a, i32 b) {
+    return qmr[a] != qmr[b] ? qmr[a] < qmr[b] : colex[a] < colex[b];
+  });
+  std::vector<i32> qrank(Q);
+  for (i64 p = 0; p < Q; ++p) qrank[ord[p]] = (i32)(E + T + p);
+  // packed triangle key v0 + v1<<16 + v2<<32 (n < 65536)
+  std::unordered_map<u64, i32> tkey;
+  tkey.reserve(T * 2);
+  auto pack = [](u64 a, u64 b, u64 c) { return a | (b << 16) | (c << 32); };
+  std::vector<i32> tpos(T);  // triangle index -> local column index (global - E)
+  for (i64 k = 0; k < T; ++k) {
+    tkey[pack(tr.v0[k], tr.v1[k], tr.v2[k])] = (i32)k;
+    tpos[k] = tr.grank[k] - (i32)E;
+  }
+  std::vector<std::vector<i32>> cof(T);  // by local triangle column index
+  for (i64 k = 0; k < Q; ++k) {
+    u64 a = q0[k], b = q1[k], c = q2[k], d = q3[k];
+    u64 f[4] = {pack(a, b, c), pack(a, b, d), pack(a, c, d), pack(b, c, d)};
+    for (int z = 0; z < 4; ++z) cof[tpos[tkey.at(f[z])]].push_back(qrank[k]);
+  }
+  for (auto& r : cof) std::sort(r.begin(), r.end());
+  // rank -> filtration value over edges, triangles, tetrahedra
+  std::vector<float> r2f(edge_filt);
+  for (i64 p = 0; p < T; ++p) r2f.push_back(edge_filt[tr.mr[tr.sorted_idx[p]]]);
+  for (i64 p = 0; p < Q; ++p) r2f.push_back(edge_filt[qmr[ord[p]]]);
+  // clearing: triangles that are H1 pivots are skipped
+  std::vector<char> skip(T, 0);
+  for (i32 piv : R.h1_all_pivots) skip[piv - E] = 1;
+  std::vector<i32> cmf(E + T + Q, -1);
+  for (i64 c = 0; c < T; ++c) {
+    if (skip[c]) continue;
+    for (i32 t : cof[c]) cmf[t] = std::max(cmf[t], (i32)(E + c));
+  }
+  std::map<i32, Col> table;
+  Col cur, tmp;
+  for (i64 c = T - 1; c >= 0; --c) {
+    if (skip[c]) continue;
+    const i32 r = (i32)(E + c);
+    if (cof[c].empty()) {
+      R.h2_ess.push_back(r);
+      continue;
+    }
+    i32 young = cof[c][0];
+    if (cmf[young] == r) {
+      table[young] = cof[c];
+      if (r2f[young] > r2f[r]) {
+        R.h2_births.push_back(r);
+        R.h2_deaths.push_back(young);
+      }
+      continue;
+    }
+    cur = cof[c];
+    while (!cur.empty()) {
+      auto it = table.find(cur[0]);
+      if (it == table.end()) break;
+      xor_into(cur, it->second, tmp);
+    }
+    if (!cur.empty()) {
+      table[cur[0]] = cur;
+      if (r2f[cur[0]] > r2f[r]) {
+        R.h2_births.push_back(r);
+        R.h2_deaths.push_back(cur[0]);
+      }
+    } else {
+      R.h2_ess.push_back(r);
+    }
+  }
+  for (size_t k = 0; k < R.h2_births.size(); ++k) {
+    R.h2.push_back(r2f[R.h2_births[k]]);
+    R.h2.push_back(r2f[R.h2_deaths[k]]);
+  }
+  for (i32 r : R.h2_ess) {
+    R.h2.push_back(r2f[r]);
+    R.h2.push_back(INFINITY);
+  }
+  stable_sort_rows_by_birth(R.h2);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Squared threshold as the reference forms it: double product, then FP32
+// (rips.py:125; the kernel argument is an fp32 scalar).
+float oracle_threshold_sq(double max_edge_length) {
+  return (float)(max_edge_length * max_edge_length);
+}
+
+// Full pipeline of persistence.py:77-215 for max_dim 0..2.
+// fused: 1 = dist^2 accumulated with fmaf, 0 = separate multiply and add.
+// stop_after: 0 = everything, 1 = filtration only, 2 = through H0.
+// filt_override: optional per-edge filtration values (sorted edge order, length
+// n_override == E) used instead of sqrtf(dist^2); the reference's CPU runs
+// take square roots with torch's CPU kernel, which is not always correctly
+// rounded, while torch on CUDA and the CUDA path round correctly.
+void* oracle_run(const float* pts, int64_t n, int d, double max_edge_length, int max_dim,
+                 int fused, int nthreads, int stop_after, const float* filt_override,
+                 int64_t n_override) {
+  Result* R = new Result();
+  const float thr = oracle_threshold_sq(max_edge_length);
+  if (n <= 1) {
+    if (n == 1) {
+      R->h0 = {0.0f, INFINITY};
+      R->n_components = 1;
+    }
+    return R;
+  }
+  enumerate_edges(pts, n, d, thr, fused, nthreads, R->edge_i, R->edge_j, R->edge_dsq);
+  sort_edges(R->edge_i, R->edge_j, R->edge_dsq);
+  if (stop_after == 1) return R;
+  const i64 E = (i64)R->edge_i.size();
+  boruvka(R->edge_i, R->edge_j, n, R->mst_idx, R->n_components);
+  std::vector<float> filt(E);
+  if (filt_override) {
+    if (n_override != E) {
+      R->error = "filt_override length differs from the edge count";
+      return R;
+    }
+    for (i64 e = 0; e < E; ++e) filt[e] = filt_override[e];
+  } else {
+    for (i64 e = 0; e < E; ++e) filt[e] = std::sqrt(R->edge_dsq[e]);
+  }
+  std::vector<float> deaths;
+  for (i64 e : R->mst_idx) deaths.push_back(filt[e]);
+  std::sort(deaths.begin(), deaths.end());
+  for (float x : deaths) {
+    R->h0.push_back(0.0f);
+    R->h0.push_back(x);
+  }
+  for (i64 c = 0; c < R->n_components; ++c) {
+    R->h0.push_back(0.0f);
+    R->h0.push_back(INFINITY);
+  }
+  if (stop_after == 2 || max_dim == 0) return R;
+  CSR g = vertex_csr(R->edge_i, R->edge_j, n);
+  std::vector<char> mst_mask(E, 0);
+  for (i64 e : R->mst_idx) mst_mask[e] = 1;
+  Triangles tr = enumerate_triangles(R->edge_i, R->edge_j, g);
+  h1_native(*R, n, g, tr, mst_mask, filt);
+  if (max_dim >= 2) h2_blocks(*R, g, tr, filt);
+  return R;
+}
+
+void oracle_free(void* h) { delete static_cast<Result*>(h); }
+
+// Returns a pointer to the named array and its element count (0 if empty).
+// dtype codes: 1 = int32, 2 = int64, 3 = float32.
+const void* oracle_get(void* h, const char* name, int64_t* count, int* dtype) {
+  Result* R = static_cast<Result*>(h);
+  std::string s(name);
+#define ARR(nm, vec, code)              \
+  if (s == nm) {                        \
+    *count = (int64_t)R->vec.size();    \
+    *dtype = code;                      \
+    return R->vec.data();               \
+  }
+  ARR("edge_i", edge_i, 1)
+  ARR("edge_j", edge_j, 1)
+  ARR("edge_dsq", edge_dsq, 3)
+  ARR("mst_idx", mst_idx, 2)
+  ARR("h0", h0, 3)
+  ARR("tri_max_rank_sorted", tri_max_rank_sorted, 1)
+  ARR("ap_births", ap_births, 1)
+  ARR("ap_deaths", ap_deaths, 1)
+  ARR("res_births", res_births, 1)
+  ARR("res_deaths", res_deaths, 1)
+  ARR("ess_births", ess_births, 1)
+  ARR("h1_all_pivots", h1_all_pivots, 1)
+  ARR("h1", h1, 3)
+  ARR("h2", h2, 3)
+  ARR("h2_births", h2_births, 1)
+  ARR("h2_deaths", h2_deaths, 1)
+  ARR("h2_ess", h2_ess, 1)
+#undef ARR
+  *count = -1;
+  *dtype = 0;
+  return nullptr;
+}
+
+const char* oracle_error(void* h) { return static_cast<Result*>(h)->error.c_str(); }
+
+int64_t oracle_scalar(void* h, const char* name) {
+  Result* R = static_cast<Result*>(h);
+  std::string s(name);
+  if (s == "E") return (int64_t)R->edge_i.size();
+  if (s == "n_components") return R->n_components;
+  if (s == "T") return R->T;
+  if (s == "Q") return R->Q;
+  if (s == "cofacet_nnz") return R->cofacet_nnz;
+  if (s == "n_apparent") return R->n_apparent;
+  if (s == "residual") return R->residual;
+  return -1;
+}
+
+}  // extern "C"
