@@ -136,131 +136,181 @@ int scan_impl(const In* in, Out* out, i64 n, void* ws, size_t ws_bytes, cudaStre
 }
 
 // ---------------------------------------------------------------------------
-// Radix sort
+// Radix sort: one-sweep LSD passes with decoupled look-back
 // ---------------------------------------------------------------------------
+// One kernel histograms all eight digit positions at once; a pass whose
+// digit is constant (one bin holds every key) is skipped on the device, and
+// the ping-pong parity of every pass follows from the same histogram, so the
+// host never synchronises. Each pass is one kernel: a block takes the next
+// tile ticket (tickets are handed out in launch order, so every tile a block
+// waits on belongs to a block that is already running), ranks its 4096 keys
+// stably with warp match-any, publishes its per-digit counts, and sums the
+// counts of earlier tiles by looking back until it meets a published
+// inclusive prefix. The look-back spin is bounded.
 constexpr int RS_NT = 256;
 constexpr int RS_WARPS = RS_NT / 32;
 constexpr int RS_PER_WARP = 512;
-constexpr int RS_TILE = RS_WARPS * RS_PER_WARP;  // 4096 keys per block
+constexpr int RS_TILE = RS_WARPS * RS_PER_WARP;  // 4096 keys per tile
 constexpr int RS_ROUNDS = RS_PER_WARP / 32;      // 16
+constexpr u64 LB_AGG = 1ull << 32, LB_PRE = 2ull << 32;
+constexpr int LB_SPIN_LIMIT = 1 << 24;
 
-struct SortFlags {
-  // [0..7] pass active, [8..15] active passes before this one, [16] total
-  int f[24];
-  unsigned long long or_bits, and_bits;
+struct SortCtl {
+  u32 ghist[8][256];
+  u32 ticket[8];
+  int error;
 };
 
-__global__ void k_or_and(const u64* __restrict__ keys, i64 n, SortFlags* fl) {
-  u64 o = 0, a = ~0ull;
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(RS_NT) k_os_hist(const u64* __restrict__ keys, i64 n, int p0, int p1,
+                                                  SortCtl* ctl) {
+  __shared__ u32 h[8][256];
+  for (int i = threadIdx.x; i < 8 * 256; i += RS_NT) h[i >> 8][i & 255] = 0;
+  __syncthreads();
+  for (i64 i = (i64)blockIdx.x * RS_NT + threadIdx.x; i < n; i += (i64)gridDim.x * RS_NT) {
     const u64 k = keys[i];
-    o |= k;
-    a &= k;
+    for (int p = p0; p < p1; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255u], 1u);
   }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    o |= __shfl_xor_sync(FULL, o, d);
-    a &= __shfl_xor_sync(FULL, a, d);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicOr(&fl->or_bits, (unsigned long long)o);
-    atomicAnd(&fl->and_bits, (unsigned long long)a);
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * 256; i += RS_NT) {
+    const u32 v = h[i >> 8][i & 255];
+    if (v) atomicAdd(&ctl->ghist[i >> 8][i & 255], v);
   }
 }
 
-__global__ void k_plan(SortFlags* fl, int begin_pass, int end_pass) {
-  const u64 var = fl->or_bits ^ fl->and_bits;
+// Number of active passes before `pass` and whether `pass` itself is active.
+__device__ __forceinline__ void pass_plan(const SortCtl* ctl, i64 n, int p0, int pass, int* before,
+                                          bool* active) {
   int cnt = 0;
-  for (int p = 0; p < 8; ++p) {
-    const int act = (p >= begin_pass && p < end_pass && ((var >> (8 * p)) & 0xffull)) ? 1 : 0;
-    fl->f[p] = act;
-    fl->f[8 + p] = cnt;
-    cnt += act;
+  bool act = false;
+  for (int p = p0; p <= pass; ++p) {
+    const int full = __syncthreads_or(ctl->ghist[p][threadIdx.x] == (u32)n);
+    if (p < pass) cnt += !full;
+    else act = !full;
   }
-  fl->f[16] = cnt & 1;
+  *before = cnt;
+  *active = act;
 }
 
-__global__ void __launch_bounds__(RS_NT) k_radix_hist(const u64* __restrict__ kA, const u64* __restrict__ kB,
-                                                     i64 n, int pass, const SortFlags* fl,
-                                                     u32* __restrict__ hist, int nblocks) {
-  if (!fl->f[pass]) return;
-  const u64* keys = (fl->f[8 + pass] & 1) ? kB : kA;
-  __shared__ u32 h[256];
-  h[threadIdx.x] = 0;
-  __syncthreads();
-  const int shift = 8 * pass;
-  const i64 base = (i64)blockIdx.x * RS_TILE;
-#pragma unroll 4
-  for (int k = 0; k < RS_TILE / RS_NT; ++k) {
-    const i64 i = base + (i64)k * RS_NT + threadIdx.x;
-    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
-  }
-  __syncthreads();
-  hist[(i64)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
-}
-
-__global__ void __launch_bounds__(RS_NT) k_radix_scatter(u64* __restrict__ kA, u32* __restrict__ vA,
-                                                        u64* __restrict__ kB, u32* __restrict__ vB,
-                                                        i64 n, int pass, const SortFlags* fl,
-                                                        const u32* __restrict__ offs, int nblocks) {
-  if (!fl->f[pass]) return;
-  const bool srcB = fl->f[8 + pass] & 1;
+__global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u32* vB, i64 n, int p0,
+                                                  int pass, SortCtl* ctl, unsigned long long* lb,
+                                                  i64 ntiles) {
+  int before;
+  bool active;
+  pass_plan(ctl, n, p0, pass, &before, &active);
+  if (!active) return;
+  const bool srcB = before & 1;
   const u64* ks = srcB ? kB : kA;
   const u32* vs = srcB ? vB : vA;
   u64* kd = srcB ? kA : kB;
   u32* vd = srcB ? vA : vB;
   const int shift = 8 * pass;
+  const u64 epoch = (u64)(pass + 1) << 40;
   __shared__ u32 cnt[RS_WARPS][256];
-  for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_NT) cnt[i / 256][i % 256] = 0;
-  __syncthreads();
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const i64 wbase = (i64)blockIdx.x * RS_TILE + (i64)w * RS_PER_WARP;
-  u64 key[RS_ROUNDS];
-  u32 val[RS_ROUNDS], dig[RS_ROUNDS], pos[RS_ROUNDS];
-  const u32 lt = lanemask_lt();
-#pragma unroll
-  for (int r = 0; r < RS_ROUNDS; ++r) {
-    const i64 i = wbase + r * 32 + lane;
-    const bool ok = i < n;
-    const u64 k = ok ? ks[i] : 0ull;
-    const u32 v = ok ? vs[i] : 0u;
-    const u32 d = ok ? (u32)((k >> shift) & 255u) : 256u;
-    const u32 peers = __match_any_sync(FULL, d);
-    const u32 rank = __popc(peers & lt);
-    const u32 b = (d < 256u) ? cnt[w][d] : 0u;
-    __syncwarp();
-    if (d < 256u && rank == 0) cnt[w][d] = b + __popc(peers);
-    __syncwarp();
-    key[r] = k;
-    val[r] = v;
-    dig[r] = d;
-    pos[r] = b + rank;
-  }
-  __syncthreads();
+  __shared__ u32 gstart[256];
+  __shared__ u32 tbase[256];
+  __shared__ u32 wsum[RS_WARPS];
+  __shared__ i64 tile_sh;
+  // exclusive scan of the global digit counts of this pass
   {
-    u32 run = 0;
+    const u32 v = ctl->ghist[pass][threadIdx.x];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    u32 x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 y = __shfl_up_sync(FULL, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    u32 wp = 0;
+    for (int k = 0; k < w; ++k) wp += wsum[k];
+    gstart[threadIdx.x] = wp + x - v;
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const u32 lt = lanemask_lt();
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) tile_sh = atomicAdd(&ctl->ticket[pass], 1u);
+    for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_NT) cnt[i >> 8][i & 255] = 0;
+    __syncthreads();
+    const i64 tile = tile_sh;
+    if (tile >= ntiles) break;
+    const i64 wbase = tile * RS_TILE + (i64)w * RS_PER_WARP;
+    u64 key[RS_ROUNDS];
+    u32 val[RS_ROUNDS], dig[RS_ROUNDS], pos[RS_ROUNDS];
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const i64 i = wbase + r * 32 + lane;
+      const bool ok = i < n;
+      const u64 k = ok ? ks[i] : 0ull;
+      const u32 v = ok ? vs[i] : 0u;
+      const u32 d = ok ? (u32)((k >> shift) & 255u) : 256u;
+      const u32 peers = __match_any_sync(FULL, d);
+      const u32 rank = __popc(peers & lt);
+      const u32 b = (d < 256u) ? cnt[w][d] : 0u;
+      __syncwarp();
+      if (d < 256u && rank == 0) cnt[w][d] = b + __popc(peers);
+      __syncwarp();
+      key[r] = k;
+      val[r] = v;
+      dig[r] = d;
+      pos[r] = b + rank;
+    }
+    __syncthreads();
+    // per-digit tile total; warp counts become exclusive offsets within the tile
+    const int dgt = threadIdx.x;
+    u32 total = 0;
 #pragma unroll
     for (int ww = 0; ww < RS_WARPS; ++ww) {
-      const u32 c = cnt[ww][threadIdx.x];
-      cnt[ww][threadIdx.x] = run;
-      run += c;
+      const u32 c = cnt[ww][dgt];
+      cnt[ww][dgt] = total;
+      total += c;
     }
-  }
-  __syncthreads();
+    volatile unsigned long long* slot = lb + tile * 256 + dgt;
+    if (tile == 0) {
+      *slot = epoch | LB_PRE | total;
+      tbase[dgt] = gstart[dgt];
+    } else {
+      *slot = epoch | LB_AGG | total;
+      u32 excl = 0;
+      i64 t = tile - 1;
+      int spins = 0;
+      while (t >= 0) {
+        const volatile unsigned long long* vp = lb + t * 256 + dgt;
+        const unsigned long long cur = *vp;
+        if ((cur & ~((1ull << 40) - 1)) != epoch || ((cur >> 32) & 0xffull) == 0) {
+          if (++spins > LB_SPIN_LIMIT) {
+            atomicExch(&ctl->error, 1);
+            break;
+          }
+          __nanosleep(32);
+          continue;
+        }
+        excl += (u32)(cur & 0xffffffffull);
+        if (cur & LB_PRE) break;
+        --t;
+      }
+      *slot = epoch | LB_PRE | (excl + total);
+      tbase[dgt] = gstart[dgt] + excl;
+    }
+    __syncthreads();
 #pragma unroll
-  for (int r = 0; r < RS_ROUNDS; ++r) {
-    const u32 d = dig[r];
-    if (d < 256u) {
-      const u64 o = (u64)offs[(i64)d * nblocks + blockIdx.x] + cnt[w][d] + pos[r];
-      kd[o] = key[r];
-      vd[o] = val[r];
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const u32 d = dig[r];
+      if (d < 256u) {
+        const u64 o = (u64)tbase[d] + cnt[w][d] + pos[r];
+        kd[o] = key[r];
+        vd[o] = val[r];
+      }
     }
   }
 }
 
-__global__ void k_copy_back(u64* __restrict__ kA, u32* __restrict__ vA, const u64* __restrict__ kB,
-                            const u32* __restrict__ vB, i64 n, const SortFlags* fl) {
-  if (!fl->f[16]) return;
+__global__ void k_os_finish(u64* __restrict__ kA, u32* __restrict__ vA, const u64* __restrict__ kB,
+                            const u32* __restrict__ vB, i64 n, int p0, int p1, const SortCtl* ctl) {
+  int act = 0;
+  for (int p = p0; p < p1; ++p) act += !__syncthreads_or(ctl->ghist[p][threadIdx.x] == (u32)n);
+  if (!(act & 1)) return;
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
     kA[i] = kB[i];
     vA[i] = vB[i];
@@ -285,42 +335,39 @@ int scan_exclusive_u8_i32(const uint8_t* in, i32* out, i64 n, void* ws, size_t w
 }
 
 size_t radix_sort_workspace_bytes(i64 n) {
-  const i64 nblocks = (n + RS_TILE - 1) / RS_TILE + 1;
-  const i64 nh = 256 * nblocks;
-  return Carve::need((size_t)n * 8) + Carve::need((size_t)n * 4) + Carve::need((size_t)(nh + 1) * 4) +
-         scan_workspace_bytes(nh) + Carve::need(sizeof(SortFlags));
+  const i64 ntiles = (n + RS_TILE - 1) / RS_TILE + 1;
+  return Carve::need((size_t)n * 8) + Carve::need((size_t)n * 4) + Carve::need(sizeof(SortCtl)) +
+         Carve::need((size_t)ntiles * 256 * 8);
 }
 
 int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, void* ws,
                      size_t ws_bytes, cudaStream_t s) {
-  if (n < 0 || n >= (i64(1) << 31) || begin_bit < 0 || end_bit > 64 || begin_bit % 8 || end_bit % 8)
+  if (n < 0 || n >= (i64(1) << 31) || begin_bit < 0 || end_bit > 64 || begin_bit % 8 || end_bit % 8 ||
+      begin_bit > end_bit)
     return PH_ERR_ARG;
-  if (n <= 1) return PH_OK;
-  const int nblocks = (int)((n + RS_TILE - 1) / RS_TILE);
-  const i64 nh = (i64)256 * nblocks;
+  if (n <= 1 || begin_bit == end_bit) return PH_OK;
+  const i64 ntiles = (n + RS_TILE - 1) / RS_TILE;
   Carve c(ws, ws_bytes);
   u64* kB = c.take<u64>(n);
   u32* vB = c.take<u32>(n);
-  u32* offs = c.take<u32>(nh + 1);
-  void* sws = c.take<char>((i64)scan_workspace_bytes(nh));
-  SortFlags* fl = c.take<SortFlags>(1);
-  if (!kB || !vB || !offs || !sws || !fl) return PH_ERR_ARG;
-  cudaMemsetAsync(fl, 0, sizeof(SortFlags), s);
-  cudaMemsetAsync(&fl->and_bits, 0xff, sizeof(unsigned long long), s);
-  const int g = (int)std::min<i64>((n + 255) / 256, 1184);
+  SortCtl* ctl = c.take<SortCtl>(1);
+  unsigned long long* lb = c.take<unsigned long long>(ntiles * 256);
+  if (!kB || !vB || !ctl || !lb) return PH_ERR_ARG;
+  // ctl and lb are adjacent in the workspace: one memset clears both
+  const size_t clear = (size_t)((char*)(lb + ntiles * 256) - (char*)ctl);
+  cudaMemsetAsync(ctl, 0, clear, s);
+  const int p0 = begin_bit / 8, p1 = end_bit / 8;
+  const int gh = (int)std::max<i64>(1, std::min<i64>((n + RS_NT * 16 - 1) / (RS_NT * 16), 296));
   ph::count_launch();
-  k_or_and<<<g, 256, 0, s>>>(keys, n, fl);
-  ph::count_launch();
-  k_plan<<<1, 1, 0, s>>>(fl, begin_bit / 8, end_bit / 8);
-  for (int p = begin_bit / 8; p < end_bit / 8; ++p) {
+  k_os_hist<<<gh, RS_NT, 0, s>>>(keys, n, p0, p1, ctl);
+  const int gp = (int)std::min<i64>(ntiles, 148 * 4);
+  for (int p = p0; p < p1; ++p) {
     ph::count_launch();
-    k_radix_hist<<<nblocks, RS_NT, 0, s>>>(keys, kB, n, p, fl, offs, nblocks);
-    PH_TRY((scan_impl<u32, u32>(offs, offs, nh, sws, scan_workspace_bytes(nh), s, &fl->f[p])));
-    ph::count_launch();
-    k_radix_scatter<<<nblocks, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p, fl, offs, nblocks);
+    k_os_pass<<<gp, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
   }
+  const int gf = (int)std::max<i64>(1, std::min<i64>((n + 255) / 256, 1184));
   ph::count_launch();
-  k_copy_back<<<g, 256, 0, s>>>(keys, vals, kB, vB, n, fl);
+  k_os_finish<<<gf, 256, 0, s>>>(keys, vals, kB, vB, n, p0, p1, ctl);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

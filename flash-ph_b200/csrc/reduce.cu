@@ -7,58 +7,64 @@
 // Columns c = 0..K-1 are processed in the reference's order, descending c;
 // the pivot of a column is its smallest row (cofacet rank). The serial
 // algorithm adds to a column the stored column that owns its pivot until the
-// pivot is unowned. The pivot of every reduced column does not depend on the
+// pivot is unowned. The pivots of the reduced matrix do not depend on the
 // order of additions as long as a column only ever receives columns processed
 // before it (larger c): the result is always R = D V with V upper triangular,
-// and the pivots of a reduced R are unique. The GPU reducer uses that freedom
-// and proceeds in synchronous rounds over all residual columns at once:
-//   claim  : each column whose pivot changed does atomicMax(owner[pivot], c)
-//   reduce : each column that does not own its pivot adds the owner's column
-//            (owners are never written during this phase, so every read is
-//            of a stable column) and so strictly raises its pivot
-// until a round changes nothing. Then every pivot has exactly one column, so
-// the pairs and the essential (emptied) columns are the serial ones, bit for
-// bit. Apparent columns own their pivot from the start and never change:
-// no column processed before an apparent column can ever contain its pivot.
-// Merged columns live in a bump-allocated pool; running out of pool or of the
-// round budget sets a status code, no wait is unbounded.
-#include <cooperative_groups.h>
-
+// and the pivots (hence the pairs and the set of emptied columns) of any such
+// reduced R are unique. The GPU reducer uses that freedom and runs lock-free:
+// each warp takes a residual column, keeps it in shared memory and adds the
+// column that owns its current pivot while that owner is a larger column.
+// When the pivot is free or held by a smaller column, the warp publishes the
+// column (immutable pool copy, then its descriptor, then a fence) and claims
+// the pivot with atomicMax. A smaller column it displaces is taken over by the
+// same warp and reduced further. No warp ever waits for another; every loop
+// is bounded; running out of pool sets a status code. Apparent columns own
+// their pivot from the start and are never displaced (no column processed
+// before an apparent column can contain its pivot).
 #include <algorithm>
 #include <climits>
 
 #include "prim.cuh"
 
-namespace cg = cooperative_groups;
-
 namespace ph {
 namespace {
 
 constexpr int RD_NT = 256;
+constexpr int RD_WARPS = RD_NT / 32;
+constexpr int RD_CAP = 512;  // per-warp shared buffer (entries)
+constexpr unsigned FULL = 0xffffffffu;
+constexpr u64 D_CSR = 1ull << 63;
+constexpr u64 D_OFF = (1ull << 40) - 1;
+constexpr int D_LEN_MAX = (1 << 23) - 1;
 
 struct RedCtl {
   int nres;
-  int last_change_round;
+  int next;
   int abort;
-  int rounds;
+  int pad;
   unsigned long long pool_top;
+  unsigned long long merges;
+  unsigned long long takeovers;
 };
 
-// Column content: desc >= 0 -> pool offset; desc < 0 -> cofacet CSR offset -(desc+1).
-__device__ __forceinline__ const i32* col_ptr(i64 desc, const i32* cof, const i32* pool) {
-  return desc >= 0 ? pool + desc : cof + (-(desc + 1));
+// Column descriptor: bit 63 = content in the cofacet CSR (else in the pool),
+// bits 40..62 = length, bits 0..39 = offset.
+__device__ __forceinline__ u64 pack_desc(bool csr, u64 len, u64 off) {
+  return (csr ? D_CSR : 0ull) | (len << 40) | off;
+}
+__device__ __forceinline__ int dlen(u64 d) { return (int)((d >> 40) & (u64)D_LEN_MAX); }
+__device__ __forceinline__ const i32* dptr(u64 d, const i32* cof, const i32* pool) {
+  return ((d & D_CSR) ? cof : pool) + (d & D_OFF);
 }
 
 __global__ void k_classify(const i32* __restrict__ off, const i32* __restrict__ cof, i64 K, i32 col_base,
                            i32 row_base, const uint8_t* __restrict__ skip, const i32* __restrict__ cmf,
                            i32* __restrict__ state, i32* __restrict__ piv, i32* __restrict__ owner,
-                           i32* __restrict__ resid, i64* __restrict__ desc, i32* __restrict__ len,
-                           uint8_t* __restrict__ changed, RedCtl* ctl) {
+                           i32* __restrict__ resid, u64* __restrict__ desc, RedCtl* ctl, int* status) {
   for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x) {
     const i32 o0 = off[c], o1 = off[c + 1];
-    desc[c] = -(i64)o0 - 1;
-    len[c] = o1 - o0;
-    changed[c] = 1;
+    if (o1 - o0 > D_LEN_MAX) set_status(status, PH_ERR_OVERFLOW);
+    desc[c] = pack_desc(true, (u64)(o1 - o0), (u64)o0);
     if (skip && skip[c]) {
       state[c] = 0;
       piv[c] = -1;
@@ -79,106 +85,238 @@ __global__ void k_classify(const i32* __restrict__ off, const i32* __restrict__ 
   }
 }
 
-__device__ __forceinline__ void rd_barrier(cg::grid_group& g) {
-  if (gridDim.x == 1) __syncthreads();
-  else g.sync();
+// Loads that must see data written by other SMs during this kernel go to L2.
+template <bool G>
+__device__ __forceinline__ i32 ld(const i32* p) {
+  if (G) return __ldcg(p);
+  return *p;
 }
 
-__global__ void __launch_bounds__(RD_NT) k_reduce_rounds(const i32* __restrict__ cof, i32 row_base,
-                                                        const i32* __restrict__ resid, i32* __restrict__ piv,
-                                                        i32* owner, i64* desc, i32* len, uint8_t* changed,
-                                                        i32* pool, i64 pool_cap, RedCtl* ctl, int* status,
-                                                        int max_rounds) {
-  cg::grid_group g = cg::this_grid();
-  const i64 tid = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-  const i64 nth = (i64)gridDim.x * blockDim.x;
-  const i64 nres = ctl->nres;
-  if (tid == 0) ctl->last_change_round = -1;
-  rd_barrier(g);
-  int round = 0;
-  for (;; ++round) {
-    if (round >= max_rounds) {
-      if (tid == 0) set_status(status, PH_ERR_ITER_LIMIT);
-      break;
-    }
-    // claim
-    for (i64 r = tid; r < nres; r += nth) {
-      const i32 c = resid[r];
-      if (changed[c] && len[c] > 0) atomicMax(&owner[piv[c] - row_base], c);
-    }
-    rd_barrier(g);
-    // reduce
-    for (i64 r = tid; r < nres; r += nth) {
-      const i32 c = resid[r];
-      const i32 lc = len[c];
-      if (lc == 0) {
-        changed[c] = 0;
-        continue;
-      }
-      const i32 o = owner[piv[c] - row_base];
-      if (o == c) {
-        changed[c] = 0;
-        continue;
-      }
-      if (o < 0) {  // every pivot is claimed before this phase; never taken
-        set_status(status, PH_ERR_ARG);
-        ctl->abort = 1;
-        continue;
-      }
-      const i32 lo = len[o];
-      const i32* A = col_ptr(desc[c], cof, pool);
-      const i32* B = col_ptr(desc[o], cof, pool);
-      const unsigned long long need = (unsigned long long)lc + (unsigned long long)lo;
-      const unsigned long long at = atomicAdd(&ctl->pool_top, need);
-      if (at + need > (unsigned long long)pool_cap) {
-        set_status(status, PH_ERR_POOL);
-        ctl->abort = 1;
-        continue;
-      }
-      i32* out = pool + at;
-      int ia = 0, ib = 0, k = 0;
-      while (ia < lc && ib < lo) {
-        const i32 x = A[ia], y = B[ib];
-        if (x < y) {
-          out[k++] = x;
-          ++ia;
-        } else if (y < x) {
-          out[k++] = y;
-          ++ib;
-        } else {
-          ++ia;
-          ++ib;
-        }
-      }
-      while (ia < lc) out[k++] = A[ia++];
-      while (ib < lo) out[k++] = B[ib++];
-      desc[c] = (i64)at;
-      len[c] = k;
-      piv[c] = k ? out[0] : -1;
-      changed[c] = 1;
-      ctl->last_change_round = round;
-    }
-    rd_barrier(g);
-    if (ctl->abort || ctl->last_change_round != round) break;
+template <bool G>
+__device__ __forceinline__ int lower_bound_t(const i32* a, int n, i32 x) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ld<G>(a + mid) < x) lo = mid + 1;
+    else hi = mid;
   }
-  if (tid == 0) ctl->rounds = round + 1;
+  return lo;
 }
 
-__global__ void k_finish(const i32* __restrict__ resid, const i32* __restrict__ len, i32* __restrict__ state,
-                         i32* __restrict__ piv, const RedCtl* ctl, i64* info) {
+// out = A xor B for sorted lists of distinct ranks, computed by the whole
+// warp: every element looks itself up in the other list; a surviving a_i
+// goes to position i + lower_bound_B(a_i) - 2 * #(a_k in B, k < i), and
+// symmetrically for B. Returns the (warp-uniform) output length.
+template <bool AG, bool BG>
+__device__ int warp_symdiff(const i32* A, int na, const i32* B, int nb, i32* out) {
+  const int lane = threadIdx.x & 31;
+  const u32 lt = lanemask_lt();
+  int common = 0;
+  for (int base = 0; base < na; base += 32) {
+    const int i = base + lane;
+    bool in = false;
+    int lb = 0;
+    i32 x = 0;
+    if (i < na) {
+      x = ld<AG>(A + i);
+      lb = lower_bound_t<BG>(B, nb, x);
+      in = lb < nb && ld<BG>(B + lb) == x;
+    }
+    const u32 m = __ballot_sync(FULL, in);
+    const int ci = common + __popc(m & lt);
+    if (i < na && !in) out[i + lb - 2 * ci] = x;
+    common += __popc(m);
+  }
+  int cb = 0;
+  for (int base = 0; base < nb; base += 32) {
+    const int j = base + lane;
+    bool in = false;
+    int la = 0;
+    i32 y = 0;
+    if (j < nb) {
+      y = ld<BG>(B + j);
+      la = lower_bound_t<AG>(A, na, y);
+      in = la < na && ld<AG>(A + la) == y;
+    }
+    const u32 m = __ballot_sync(FULL, in);
+    const int dj = cb + __popc(m & lt);
+    if (j < nb && !in) out[j + la - 2 * dj] = y;
+    cb += __popc(m);
+  }
+  return na + nb - 2 * common;
+}
+
+__device__ __forceinline__ int symdiff(const i32* A, bool ag, int na, const i32* B, bool bg, int nb, i32* out) {
+  if (ag) return bg ? warp_symdiff<true, true>(A, na, B, nb, out) : warp_symdiff<true, false>(A, na, B, nb, out);
+  return bg ? warp_symdiff<false, true>(A, na, B, nb, out) : warp_symdiff<false, false>(A, na, B, nb, out);
+}
+
+// Bump allocation in the pool (lane 0), broadcast to the warp; ~0 on overflow.
+__device__ __forceinline__ unsigned long long pool_alloc(RedCtl* ctl, i64 cap, int n, int* status) {
+  unsigned long long at = 0;
+  if ((threadIdx.x & 31) == 0) {
+    at = atomicAdd(&ctl->pool_top, (unsigned long long)n);
+    if (at + (unsigned long long)n > (unsigned long long)cap) {
+      set_status(status, PH_ERR_POOL);
+      atomicExch(&ctl->abort, 1);
+      at = ~0ull;
+    }
+  }
+  return __shfl_sync(FULL, at, 0);
+}
+
+__global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i32 row_base,
+                                                 const i32* __restrict__ resid, u64* desc, i32* owner, i32* pool,
+                                                 i64 pool_cap, RedCtl* ctl, int* status, int max_steps) {
+  __shared__ i32 sW[RD_WARPS][2][RD_CAP];
+  __shared__ i32 sB[RD_WARPS][RD_CAP];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nres = ctl->nres;
+  volatile u64* vdesc = desc;
+  volatile i32* vowner = owner;
+  volatile int* vabort = &ctl->abort;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(&ctl->next, 1);
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= nres || *vabort) break;
+    i32 c = resid[idx];
+    u64 dc = vdesc[c];
+    // working column: shared buffer sW[w][cur] or, when too long, global
+    int cur = 0;
+    int k = dlen(dc);
+    const i32* W;
+    bool wg;          // W is in global memory
+    bool published;   // dc describes W exactly (nothing to write before a claim)
+    auto load_work = [&](u64 d) {
+      k = dlen(d);
+      const i32* src = dptr(d, cof, pool);
+      if (k <= RD_CAP) {
+        for (int i = lane; i < k; i += 32) sW[w][cur][i] = __ldcg(src + i);
+        __syncwarp();
+        W = sW[w][cur];
+        wg = false;
+      } else {
+        W = src;
+        wg = true;
+      }
+      dc = d;
+      published = true;
+    };
+    load_work(dc);
+    for (int step = 0;; ++step) {
+      if (step >= max_steps) {
+        if (lane == 0) set_status(status, PH_ERR_ITER_LIMIT);
+        atomicExch(&ctl->abort, 1);
+        break;
+      }
+      if (k == 0) {
+        if (lane == 0) vdesc[c] = pack_desc(false, 0, 0);
+        break;
+      }
+      const i32 p = wg ? __ldcg(W) : W[0];
+      i32 o = vowner[p - row_base];
+      if (o < c) {
+        // publish W, then claim p
+        if (!published) {
+          const unsigned long long at = pool_alloc(ctl, pool_cap, k, status);
+          if (at == ~0ull) break;
+          for (int i = lane; i < k; i += 32) pool[at + i] = wg ? __ldcg(W + i) : W[i];
+          dc = pack_desc(false, (u64)k, at);
+          published = true;
+        }
+        __threadfence();
+        __syncwarp();
+        i32 old = 0;
+        if (lane == 0) {
+          vdesc[c] = dc;
+          __threadfence();
+          old = atomicMax(&owner[p - row_base], c);
+        }
+        old = __shfl_sync(FULL, old, 0);
+        if (old < c) {
+          if (old < 0) break;  // claimed a free pivot: this work item is done
+          // displaced a smaller column: take it over
+          if (lane == 0) atomicAdd(&ctl->takeovers, 1ull);
+          c = old;
+          __threadfence();
+          load_work(vdesc[c]);
+          continue;
+        }
+        o = old;  // a larger column got there first
+      }
+      if (o == c) {  // cannot happen: a column never owns a pivot it is still reducing
+        if (lane == 0) set_status(status, PH_ERR_ARG);
+        break;
+      }
+      // add the larger owner o
+      __threadfence();
+      const u64 od = vdesc[o];
+      const int lb = dlen(od);
+      const i32* Bsrc = dptr(od, cof, pool);
+      const i32* B;
+      bool bg;
+      if (lb <= RD_CAP) {
+        for (int i = lane; i < lb; i += 32) sB[w][i] = __ldcg(Bsrc + i);
+        __syncwarp();
+        B = sB[w];
+        bg = false;
+      } else {
+        B = Bsrc;
+        bg = true;
+      }
+      i32* out;
+      bool og;
+      unsigned long long at = 0;
+      if (k + lb <= RD_CAP) {
+        out = sW[w][cur ^ 1];
+        og = false;
+      } else {
+        at = pool_alloc(ctl, pool_cap, k + lb, status);
+        if (at == ~0ull) break;
+        out = pool + at;
+        og = true;
+      }
+      const int m = symdiff(W, wg, k, B, bg, lb, out);
+      __syncwarp();
+      if (lane == 0) atomicAdd(&ctl->merges, 1ull);
+      k = m;
+      if (og) {
+        __threadfence();
+        W = out;
+        wg = true;
+        dc = pack_desc(false, (u64)k, at);
+        published = true;
+      } else {
+        cur ^= 1;
+        W = sW[w][cur];
+        wg = false;
+        published = false;
+      }
+    }
+  }
+}
+
+__global__ void k_finish(const i32* __restrict__ cof, const i32* __restrict__ pool, const i32* __restrict__ resid,
+                         const u64* __restrict__ desc, i32* __restrict__ state, i32* __restrict__ piv,
+                         const RedCtl* ctl, i64* info) {
   const i64 nres = ctl->nres;
   for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < nres; r += (i64)gridDim.x * blockDim.x) {
     const i32 c = resid[r];
-    if (len[c] == 0) {
+    const u64 d = desc[c];
+    if (dlen(d) == 0) {
       state[c] = 3;
       piv[c] = -1;
+    } else {
+      state[c] = 2;
+      piv[c] = dptr(d, cof, pool)[0];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && info) {
     info[0] = ctl->nres;
-    info[1] = ctl->rounds;
+    info[1] = (i64)ctl->merges;
     info[2] = (i64)ctl->pool_top;
-    info[3] = 0;
+    info[3] = (i64)ctl->takeovers;
   }
 }
 
@@ -245,7 +383,7 @@ using namespace ph;
 
 extern "C" size_t ph_reduce_workspace_bytes(int64_t K, int64_t R) {
   return Carve::need((size_t)R * 4) + Carve::need((size_t)K * 4) + Carve::need((size_t)K * 8) +
-         Carve::need((size_t)K * 4) + Carve::need((size_t)K) + Carve::need(sizeof(RedCtl));
+         Carve::need(sizeof(RedCtl));
 }
 
 extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,
@@ -255,7 +393,8 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
                          void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (K < 0 || R < 0 || pool_cap < 0) return PH_ERR_ARG;
-  if (K >= (int64_t(1) << 31) || R >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
+  if (K >= (int64_t(1) << 31) || R >= (int64_t(1) << 31) || pool_cap >= (int64_t(1) << 40))
+    return PH_ERR_OVERFLOW;
   if (K == 0) {
     if (d_info) cudaMemsetAsync(d_info, 0, 4 * sizeof(int64_t), s);
     PH_CHECK_LAUNCH();
@@ -264,40 +403,24 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   Carve c(workspace, workspace_bytes);
   i32* owner = c.take<i32>(std::max<i64>(R, 1));
   i32* resid = c.take<i32>(K);
-  i64* desc = c.take<i64>(K);
-  i32* len = c.take<i32>(K);
-  uint8_t* changed = c.take<uint8_t>(K);
+  u64* desc = c.take<u64>(K);
   RedCtl* ctl = c.take<RedCtl>(1);
-  if (!owner || !resid || !desc || !len || !changed || !ctl) return PH_ERR_ARG;
+  if (!owner || !resid || !desc || !ctl) return PH_ERR_ARG;
   cudaMemsetAsync(owner, 0xff, sizeof(i32) * std::max<i64>(R, 1), s);
   cudaMemsetAsync(ctl, 0, sizeof(RedCtl), s);
   ph::count_launch();
   k_classify<<<grid_for(K), 256, 0, s>>>(cof_off, cof_data, K, col_base, row_base, skip, row_cmf, col_state,
-                                         col_piv, owner, resid, desc, len, changed, ctl);
-  PH_CHECK_LAUNCH();
-  int max_rounds = 1 << 22;
-  // The residual count is only known on the device; size the grid for K.
-  if (K <= 4 * RD_NT) {
-    ph::count_launch();
-    k_reduce_rounds<<<1, RD_NT, 0, s>>>(cof_data, row_base, resid, col_piv, owner, desc, len, changed, pool,
-                                        pool_cap, ctl, d_status, max_rounds);
-  } else {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_reduce_rounds, RD_NT, 0);
-    if (per_sm < 1) return PH_ERR_CUDA;
-    const int blocks = (int)std::max<i64>(2, std::min<i64>((K + RD_NT * 4 - 1) / (RD_NT * 4), (i64)sms * per_sm));
-    const i32* cof = cof_data;
-    void* args[] = {(void*)&cof,     (void*)&row_base, (void*)&resid,  (void*)&col_piv, (void*)&owner,
-                    (void*)&desc,    (void*)&len,      (void*)&changed, (void*)&pool,   (void*)&pool_cap,
-                    (void*)&ctl,     (void*)&d_status, (void*)&max_rounds};
-    ph::count_launch();
-    if (cudaLaunchCooperativeKernel((const void*)k_reduce_rounds, blocks, RD_NT, args, 0, s) != cudaSuccess)
-      return PH_ERR_CUDA;
-  }
+                                         col_piv, owner, resid, desc, ctl, d_status);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // residual count is known only on the device; K bounds it
+  const int blocks = (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * 4));
   ph::count_launch();
-  k_finish<<<grid_for(K), 256, 0, s>>>(resid, len, col_state, col_piv, ctl, d_info);
+  k_reduce<<<blocks, RD_NT, 0, s>>>(cof_data, row_base, resid, desc, owner, pool, pool_cap, ctl, d_status,
+                                    1 << 24);
+  ph::count_launch();
+  k_finish<<<grid_for(K), 256, 0, s>>>(cof_data, pool, resid, desc, col_state, col_piv, ctl, d_info);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -36,7 +36,7 @@ class Triangles(NamedTuple):
 class Reduction(NamedTuple):
     state: Tensor   # (K,) int32: 0 skipped, 1 apparent, 2 paired, 3 essential
     piv: Tensor     # (K,) int32 pivot global rank or -1
-    info: Tensor    # (4,) int64 [residual, rounds, pool used, 0]
+    info: Tensor    # (4,) int64 [residual columns, column additions, pool entries used, takeovers]
     status: Tensor  # (1,) int32 device status
 
 

@@ -173,14 +173,17 @@ int ph_cof_max_face(const int32_t* faces_aos, const int32_t* f0, const int32_t* 
  * processed in the reference's order (descending rank), pivot = smallest
  * cofacet rank. Apparent pairs (the column is the largest non-skipped face of
  * its youngest cofacet) are detected first (reduce_h1_gpu.py:159-223); the
- * remaining columns are reduced on the GPU by rounds in which every column
- * whose pivot is claimed by an earlier-processed column adds that column.
- * The pivots, and so the pairs and the essential columns, are those of the
- * serial reduction (cohomology_general.py:202-371).
+ * remaining columns are reduced on the GPU lock-free, one warp per column:
+ * a column adds the column owning its pivot while that owner was processed
+ * earlier (larger index), then claims the pivot with an atomic maximum,
+ * taking over any later-processed column it displaces. The pivots, and so
+ * the pairs and the essential columns, are those of the serial reduction
+ * (cohomology_general.py:202-371).
  * col_state[c]: 0 skipped, 1 apparent, 2 reduced to a pivot, 3 essential.
  * col_piv[c]: pivot global rank (states 1 and 2) or -1.
  * pool: scratch for reduced columns, pool_cap int32 entries.
- * d_info (int64 x 4, device): [residual columns, rounds, pool entries used, 0].
+ * d_info (int64 x 4, device): [residual columns, column additions, pool
+ * entries used, takeovers].
  * d_status: PH_ERR_POOL or PH_ERR_ITER_LIMIT on failure. */
 size_t ph_reduce_workspace_bytes(int64_t K, int64_t R);
 int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,

@@ -36,6 +36,7 @@ struct Result {
   std::vector<float> h0;
   // H1 (reduce_h1_gpu.py:438-604)
   i64 T = 0, cofacet_nnz = 0, n_apparent = 0, residual = 0;
+  i64 xor_ops = 0, xor_max = 0, xor_elems = 0;  // reduction work statistics
   std::vector<i32> tri_max_rank_sorted;
   std::vector<i32> ap_births, ap_deaths, res_births, res_deaths, ess_births;
   std::vector<i32> h1_all_pivots;
@@ -419,11 +420,16 @@ void h1_native(Result& R, i64 n, const CSR& g, const Triangles& tr, const std::v
       continue;
     }
     cur = cof[e];
+    i64 ops = 0;
     while (!cur.empty()) {
       auto it = table.find(cur[0]);
       if (it == table.end()) break;
+      R.xor_elems += (i64)(cur.size() + it->second.size());
       xor_into(cur, it->second, tmp);
+      ++ops;
     }
+    R.xor_ops += ops;
+    R.xor_max = std::max(R.xor_max, ops);
     if (!cur.empty()) {
       i32 piv = cur[0];
       R.h1_all_pivots.push_back(piv);
@@ -682,6 +688,9 @@ int64_t oracle_scalar(void* h, const char* name) {
   if (s == "cofacet_nnz") return R->cofacet_nnz;
   if (s == "n_apparent") return R->n_apparent;
   if (s == "residual") return R->residual;
+  if (s == "xor_ops") return R->xor_ops;
+  if (s == "xor_max") return R->xor_max;
+  if (s == "xor_elems") return R->xor_elems;
   return -1;
 }
 

@@ -46,7 +46,7 @@ def test_pipeline_matches_oracle(name):
         assert f.edge_i.shape[0] == ref["E"]
         assert np.array_equal(f.edge_i.cpu().numpy(), ref["edge_i"])
         assert np.array_equal(f.edge_j.cpu().numpy(), ref["edge_j"])
-        assert np.array_equal(_bits(f.edge_dsq.cpu().numpy()), _bits(ref["edge_dsq"]))
+        assert np.array_equal(_bits(f.edge_dist_sq.cpu().numpy()), _bits(ref["edge_dsq"]))
     dg = rips_persistence(_fp(pts), t, max_dim=md)
     assert len(dg) == md + 1
     assert all(d.device.type == "cuda" and d.dtype == torch.float32 for d in dg)
@@ -76,13 +76,18 @@ def test_h1_pairs_and_classes_match_oracle(name):
     assert int(ncomp.item()) == ref["n_components"]
     rows, tris, red, info = h1_diagram(f, ef, mst)
     assert tris.T == ref["T"]
+    if ref["T"] == 0:  # the reference builds the rows directly; no pairs
+        assert np.array_equal(_bits(rows.cpu().numpy()), _bits(ref["h1"]))
+        return
     state = red.state.cpu().numpy()
     piv = red.piv.cpu().numpy()
     E = ref["E"]
     assert int((state == 1).sum()) == ref["n_apparent"]
     assert int((state == 0).sum()) == len(ref["mst_idx"])
-    # the reference's residual count includes columns without cofacets
-    assert int((state != 0).sum()) - int((state == 1).sum()) == ref["residual"]
+    # the reference's residual count includes columns without cofacets (and is
+    # not computed at all when there are no triangles)
+    if ref["T"] > 0:
+        assert int((state != 0).sum()) - int((state == 1).sum()) == ref["residual"]
     assert int(info[0]) <= ref["residual"]
     # every pair of the oracle appears with the same pivot
     for b, dth in zip(ref["ap_births"], ref["ap_deaths"]):

@@ -1,0 +1,66 @@
+"""GPU checks of the filtration-sort and adjacency entry points on random
+inputs at tile-boundary sizes, against numpy stable sorts."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_edges(E, n, seed):
+    rng = np.random.default_rng(seed)
+    # distinct pairs i < j
+    flat = rng.choice(n * (n - 1) // 2, size=E, replace=False)
+    j = np.floor((1 + np.sqrt(1 + 8 * flat.astype(np.float64))) / 2).astype(np.int64)
+    j = np.where(j * (j - 1) // 2 > flat, j - 1, j)
+    j = np.where((j + 1) * j // 2 <= flat, j + 1, j)
+    i = flat - j * (j - 1) // 2
+    assert np.all((0 <= i) & (i < j) & (j < n))
+    # few distinct lengths so that dist^2 ties are frequent
+    dsq = rng.integers(0, 50, size=E).astype(np.float32) / np.float32(7.0)
+    return i.astype(np.int32), j.astype(np.int32), dsq
+
+
+@pytest.mark.parametrize("E", [1, 2, 5, 4095, 4096, 4097, 70000, 1 << 20])
+def test_edges_sort_matches_numpy(E):
+    from flashph_b200.rips import sort_edges
+    n = 50000
+    ei, ej, ed = _random_edges(E, n, E)
+    key = (ed.view(np.uint32).astype(np.uint64) << np.uint64(32)) | (
+        (ej.astype(np.uint64) * (ej.astype(np.uint64) - np.uint64(1)) // np.uint64(2) + ei.astype(np.uint64))
+        & np.uint64(0xFFFFFFFF))
+    order = np.argsort(key, kind="stable")
+    oi, oj, od = sort_edges(torch.from_numpy(ei).cuda(), torch.from_numpy(ej).cuda(),
+                            torch.from_numpy(ed).cuda(), n)
+    assert np.array_equal(oi.cpu().numpy(), ei[order])
+    assert np.array_equal(oj.cpu().numpy(), ej[order])
+    assert np.array_equal(od.cpu().numpy().view(np.uint32), ed[order].view(np.uint32))
+
+
+@pytest.mark.parametrize("E,n", [(1, 2), (100, 1000), (5000, 300), (200000, 100000)])
+def test_vertex_csr_matches_numpy(E, n):
+    from flashph_b200.rips import vertex_csr
+    ei, ej, _ = _random_edges(E, n, 7 + E)
+    ptr, idx, rank = vertex_csr(torch.from_numpy(ei).cuda(), torch.from_numpy(ej).cuda(), n)
+    src = np.concatenate([ei, ej]).astype(np.int64)
+    dst = np.concatenate([ej, ei]).astype(np.int64)
+    rk = np.concatenate([np.arange(E), np.arange(E)])
+    o = np.argsort(src * n + dst, kind="stable")
+    want_ptr = np.zeros(n + 1, np.int64)
+    np.add.at(want_ptr, src + 1, 1)
+    want_ptr = np.cumsum(want_ptr)
+    assert np.array_equal(ptr.cpu().numpy(), want_ptr)
+    assert np.array_equal(idx.cpu().numpy(), dst[o])
+    assert np.array_equal(rank.cpu().numpy(), rk[o])
+
+
+def test_launch_counter_advances():
+    from flashph_b200 import _lib
+    from flashph_b200.rips import sort_edges
+    ei, ej, ed = _random_edges(1000, 100, 3)
+    before = _lib.launch_count()
+    sort_edges(torch.from_numpy(ei).cuda(), torch.from_numpy(ej).cuda(), torch.from_numpy(ed).cuda(), 100)
+    torch.cuda.synchronize()
+    assert _lib.launch_count() > before
