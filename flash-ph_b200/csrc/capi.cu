@@ -10,6 +10,7 @@ thread_local std::string g_last_error;
 std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 void record_error(cudaError_t e) { g_last_error = cudaGetErrorString(e); }
+void record_message(const char* msg) { g_last_error = msg; }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 }  // namespace ph
 

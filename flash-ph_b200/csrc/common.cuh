@@ -31,6 +31,8 @@ __device__ __forceinline__ u32 float_bits(float f) { return __float_as_uint(f); 
 
 // Remembers the message of a failed CUDA call for ph_last_error().
 void record_error(cudaError_t e);
+// Remembers a library-side error message for ph_last_error().
+void record_message(const char* msg);
 
 // Counts kernel launches made by this library (reported by ph_launch_count()).
 void count_launch();

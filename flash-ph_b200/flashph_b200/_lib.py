@@ -34,6 +34,8 @@ _SIGS = {
     "ph_edges_enumerate": (ctypes.c_int, [P, I64, I32, F32, P, P, P, I64, P, P]),
     "ph_edges_sort_workspace_bytes": (SZ, [I64]),
     "ph_edges_sort": (ctypes.c_int, [P, P, P, I64, I64, P, P, P, P, SZ, P]),
+    "ph_edges_sort_noalloc_max_edges": (I64, []),
+    "ph_edges_sort_noalloc": (ctypes.c_int, [P, P, P, I64, I64, P, P, P, P]),
     "ph_vertex_csr_workspace_bytes": (SZ, [I64]),
     "ph_vertex_csr": (ctypes.c_int, [P, P, I64, I64, P, P, P, P, SZ, P]),
     "ph_sqrt_f32": (ctypes.c_int, [P, P, I64, P]),

@@ -68,6 +68,18 @@ int ph_edges_sort(const int32_t* in_i, const int32_t* in_j, const float* in_dsq,
                   int64_t n, int32_t* out_i, int32_t* out_j, float* out_dsq, void* workspace,
                   size_t workspace_bytes, void* stream);
 
+/* ph_edges_sort for callers that cannot allocate device memory (their HBM
+ * is owned by another allocator or a fixed budget). No counterpart in the
+ * reference. Takes only inputs and outputs; its scratch is a 13 MiB static
+ * device array held by every GPU that loads the library, so E may not exceed
+ * ph_edges_sort_noalloc_max_edges() (2^19); larger E returns PH_ERR_CAPACITY
+ * with a message in ph_last_error(). The array's device address is looked up
+ * on the first call on each device. All calls share the array: calls whose
+ * work overlaps on the GPU race and must be ordered by the caller. */
+int64_t ph_edges_sort_noalloc_max_edges(void);
+int ph_edges_sort_noalloc(const int32_t* in_i, const int32_t* in_j, const float* in_dsq, int64_t E,
+                          int64_t n, int32_t* out_i, int32_t* out_j, float* out_dsq, void* stream);
+
 /* Per-vertex adjacency with two half-edges per edge, rows sorted by
  * neighbour index, each entry carrying the edge rank (its position in the
  * sorted edge list). Replaces rips.py:53-95 _build_vertex_csr.
