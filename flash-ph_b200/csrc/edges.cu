@@ -38,14 +38,35 @@ __device__ __forceinline__ void tile_coords(i64 b, i64 nt, i64& I, i64& J) {
   J = r + (b - start(r));
 }
 
+// Finds the cloud owning work item b: the last segment with tile_off <= b.
+__device__ __forceinline__ int find_seg(const ph_cloud_seg* segs, int nsegs, i64 b) {
+  int lo = 0, hi = nsegs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (segs[mid].tile_off <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One CTA per 128 x 128 tile of one cloud's upper triangle. Single clouds
+// pass their segment by value (segs == nullptr); batches pass a device table
+// of ph_cloud_seg records, ordered by tile_off. Vertex indices are written
+// as global indices (vbase + local).
 __global__ void __launch_bounds__(ENT, 2)
-    k_edges(const float* __restrict__ pts, i64 n, int d, float thr_sq, i64 nt,
-            i32* __restrict__ oi, i32* __restrict__ oj, float* __restrict__ od, i64 cap,
-            unsigned long long* __restrict__ count) {
+    k_edges(const float* __restrict__ pts_all, const ph_cloud_seg* __restrict__ segs, int nsegs,
+            ph_cloud_seg seg0, i32* __restrict__ oi, i32* __restrict__ oj, float* __restrict__ od,
+            i64 cap, unsigned long long* __restrict__ count) {
   __shared__ __align__(16) float xs[EK][ET];
   __shared__ __align__(16) float ys[EK][ET];
+  const ph_cloud_seg sg = segs ? segs[find_seg(segs, nsegs, (i64)blockIdx.x)] : seg0;
+  const float* __restrict__ pts = pts_all + sg.pt_off;
+  const i64 n = sg.n;
+  const int d = sg.d;
+  const float thr_sq = sg.thr_sq;
+  const i64 nt = (n + ET - 1) / ET;
   i64 I, J;
-  tile_coords(blockIdx.x, nt, I, J);
+  tile_coords((i64)blockIdx.x - sg.tile_off, nt, I, J);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const i64 i0 = I * ET, j0 = J * ET;
   float acc[8][8];
@@ -114,8 +135,8 @@ __global__ void __launch_bounds__(ENT, 2)
     for (int c = 0; c < 8; ++c) {
       if ((hit >> (r * 8 + c)) & 1ull) {
         if (pos < (unsigned long long)cap) {
-          oi[pos] = (i32)(i0 + ty * 8 + r);
-          oj[pos] = (i32)(j0 + tx * 8 + c);
+          oi[pos] = (i32)(sg.vbase + i0 + ty * 8 + r);
+          oj[pos] = (i32)(sg.vbase + j0 + tx * 8 + c);
           od[pos] = acc[r][c];
         }
         ++pos;
@@ -226,9 +247,34 @@ extern "C" int ph_edges_enumerate(const float* pts, int64_t n, int32_t d, float 
     const i64 nt = (n + ET - 1) / ET;
     const i64 tiles = nt * (nt + 1) / 2;
     if (tiles >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
+    ph_cloud_seg seg{};
+    seg.n = (int32_t)n;
+    seg.d = d;
+    seg.thr_sq = thr_sq;
     ph::count_launch();
-    k_edges<<<(unsigned)tiles, ENT, 0, s>>>(pts, n, d, thr_sq, nt, out_i, out_j, out_dsq, capacity,
-                                            d_count);
+    k_edges<<<(unsigned)tiles, ENT, 0, s>>>(pts, nullptr, 1, seg, out_i, out_j, out_dsq, capacity, d_count);
+  }
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int64_t ph_cloud_tiles(int64_t n) {
+  if (n < 2) return 0;
+  const i64 nt = (n + ET - 1) / ET;
+  return nt * (nt + 1) / 2;
+}
+
+extern "C" int ph_batch_edges_enumerate(const float* pts, const ph_cloud_seg* segs, int32_t nsegs,
+                                        int64_t ntiles, int32_t* out_i, int32_t* out_j, float* out_dsq,
+                                        int64_t capacity, unsigned long long* d_count, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nsegs < 0 || ntiles < 0 || capacity < 0 || !d_count) return PH_ERR_ARG;
+  if (ntiles >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
+  cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  if (nsegs > 0 && ntiles > 0) {
+    ph::count_launch();
+    k_edges<<<(unsigned)ntiles, ENT, 0, s>>>(pts, segs, nsegs, ph_cloud_seg{}, out_i, out_j, out_dsq, capacity,
+                                             d_count);
   }
   PH_CHECK_LAUNCH();
   return PH_OK;

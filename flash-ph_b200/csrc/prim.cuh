@@ -21,6 +21,13 @@ size_t radix_sort_workspace_bytes(i64 n);
 int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, void* ws,
                      size_t ws_bytes, cudaStream_t s);
 
+// Persistence rows in the reference's order without a sort (batch.cu);
+// col_off (nsegs+1 column offsets) may be null for a single segment.
+size_t rows_nosort_workspace_bytes(i64 K);
+int rows_nosort(const i32* state, const i32* piv, i64 K, i32 row_base, const float* filt, const i32* col_m,
+                const i32* row_m, const i64* col_off, int nsegs, float* out_rows, i64* row_off, i64* d_nrows,
+                void* ws, size_t ws_bytes, cudaStream_t s);
+
 // Workspace carving helper: aligned bump allocation inside a caller buffer.
 struct Carve {
   char* base;

@@ -326,52 +326,6 @@ __global__ void k_mark_pivots(const i32* __restrict__ state, const i32* __restri
     if (state[c] == 1 || state[c] == 2) flag[piv[c] - row_base] = 1;
 }
 
-// Row keys: (birth bits, group, order in group); group 0 apparent pairs by
-// ascending column, 1 reduced pairs and 2 essential columns by descending
-// column; columns without a row get the largest key.
-__global__ void k_row_keys(const i32* __restrict__ state, const i32* __restrict__ piv, i64 K, i32 row_base,
-                           const float* __restrict__ filt, const i32* __restrict__ col_m,
-                           const i32* __restrict__ row_m, u64* __restrict__ keys, u32* __restrict__ vals,
-                           unsigned long long* nrows) {
-  unsigned long long cnt = 0;
-  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x) {
-    const i32 st = state[c];
-    u64 key = ~0ull;
-    if (st != 0) {
-      const float fb = filt[col_m ? col_m[c] : (i32)c];
-      bool keep = true;
-      u64 group = 2;
-      if (st == 1 || st == 2) {
-        const float fd = filt[row_m[piv[c] - row_base]];
-        keep = fd > fb;
-        group = (st == 1) ? 0 : 1;
-      }
-      if (keep) {
-        const u64 ord = group == 0 ? (u64)c : (u64)(K - 1 - c);
-        key = ((u64)float_bits(fb) << 32) | (group << 30) | ord;
-        ++cnt;
-      }
-    }
-    keys[c] = key;
-    vals[c] = (u32)c;
-  }
-  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(nrows, cnt);
-}
-
-__global__ void k_rows_out(const u32* __restrict__ vals, const i32* __restrict__ state,
-                           const i32* __restrict__ piv, i32 row_base, const float* __restrict__ filt,
-                           const i32* __restrict__ col_m, const i32* __restrict__ row_m,
-                           const unsigned long long* nrows, float* __restrict__ rows, i64* d_nrows) {
-  const i64 n = (i64)*nrows;
-  for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (i64)gridDim.x * blockDim.x) {
-    const i32 c = (i32)vals[p];
-    rows[2 * p] = filt[col_m ? col_m[c] : c];
-    rows[2 * p + 1] = state[c] == 3 ? __int_as_float(0x7f800000) : filt[row_m[piv[c] - row_base]];
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *d_nrows = n;
-}
-
 inline int grid_for(i64 n, int nt = 256) {
   return (int)std::max<i64>(1, std::min<i64>((n + nt - 1) / nt, 148 * 16));
 }
@@ -438,34 +392,13 @@ extern "C" int ph_mark_pivots(const int32_t* col_state, const int32_t* col_piv, 
   return PH_OK;
 }
 
-extern "C" size_t ph_persistence_rows_workspace_bytes(int64_t K) {
-  return Carve::need((size_t)K * 8) + Carve::need((size_t)K * 4) + Carve::need(8) + radix_sort_workspace_bytes(K);
-}
+extern "C" size_t ph_persistence_rows_workspace_bytes(int64_t K) { return rows_nosort_workspace_bytes(K); }
 
 extern "C" int ph_persistence_rows(const int32_t* col_state, const int32_t* col_piv, int64_t K, int32_t row_base,
                                    const float* filt, const int32_t* col_m, const int32_t* row_m, float* out_rows,
                                    int64_t* d_nrows, void* workspace, size_t workspace_bytes, void* stream) {
-  cudaStream_t s = (cudaStream_t)stream;
   if (K < 0) return PH_ERR_ARG;
-  if (K >= (int64_t(1) << 30)) return PH_ERR_OVERFLOW;
-  if (K == 0) {
-    cudaMemsetAsync(d_nrows, 0, sizeof(int64_t), s);
-    PH_CHECK_LAUNCH();
-    return PH_OK;
-  }
-  Carve c(workspace, workspace_bytes);
-  u64* keys = c.take<u64>(K);
-  u32* vals = c.take<u32>(K);
-  unsigned long long* cnt = c.take<unsigned long long>(1);
-  void* rws = c.take<char>((i64)radix_sort_workspace_bytes(K));
-  if (!keys || !vals || !cnt || !rws) return PH_ERR_ARG;
-  cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
-  ph::count_launch();
-  k_row_keys<<<grid_for(K), 256, 0, s>>>(col_state, col_piv, K, row_base, filt, col_m, row_m, keys, vals, cnt);
-  PH_TRY(radix_sort_pairs(keys, vals, K, 0, 64, rws, radix_sort_workspace_bytes(K), s));
-  ph::count_launch();
-  k_rows_out<<<grid_for(K), 256, 0, s>>>(vals, col_state, col_piv, row_base, filt, col_m, row_m, cnt, out_rows,
-                                         d_nrows);
-  PH_CHECK_LAUNCH();
-  return PH_OK;
+  if (K >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
+  return rows_nosort(col_state, col_piv, K, row_base, filt, col_m, row_m, nullptr, 1, out_rows, nullptr, d_nrows,
+                     workspace, workspace_bytes, (cudaStream_t)stream);
 }

@@ -100,16 +100,16 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
                                                const i64* __restrict__ tri_off, const i32* __restrict__ tw,
                                                const i32* __restrict__ tfa, const i32* __restrict__ tfb,
                                                const i32* __restrict__ aptr, const i32* __restrict__ aidx,
-                                               const i32* __restrict__ arank, i32* __restrict__ tet_cnt,
-                                               const i64* __restrict__ tet_off, i32* __restrict__ qm,
-                                               i32* __restrict__ qf, int* status) {
+                                               const i32* __restrict__ arank, const uint8_t* __restrict__ enable,
+                                               i32* __restrict__ tet_cnt, const i64* __restrict__ tet_off,
+                                               i32* __restrict__ qm, i32* __restrict__ qf, int* status) {
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
   const u32 lt = lanemask_lt();
   for (i64 m = warp; m < E; m += nwarps) {
     const i64 t0 = tri_off[m], t1 = tri_off[m + 1];
-    const int nw = (int)(t1 - t0);
+    const int nw = (enable && !enable[m]) ? 0 : (int)(t1 - t0);
     i64 out = EMIT ? tet_off[m] : 0;
     int cnt = 0;
     for (int i = 0; i + 1 < nw; ++i) {
@@ -266,7 +266,8 @@ extern "C" size_t ph_tets_count_workspace_bytes(int64_t E) {
 
 extern "C" int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64_t E,
                              const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
-                             int64_t* tet_off, void* workspace, size_t workspace_bytes, void* stream) {
+                             const uint8_t* edge_enable, int64_t* tet_off, void* workspace,
+                             size_t workspace_bytes, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (E < 0) return PH_ERR_ARG;
   Carve c(workspace, workspace_bytes);
@@ -276,7 +277,8 @@ extern "C" int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64
   if (E > 0)
     ph::count_launch();
     k_tets<false><<<warp_grid(E), SX_NT, 0, s>>>(nullptr, nullptr, E, tri_off, tri_w, nullptr, nullptr, adj_ptr,
-                                                 adj_idx, adj_rank, qc, nullptr, nullptr, nullptr, nullptr);
+                                                 adj_idx, adj_rank, edge_enable, qc, nullptr, nullptr, nullptr,
+                                                 nullptr);
   PH_TRY(scan_exclusive_i32_i64(qc, tet_off, E, sws, scan_workspace_bytes(E), s));
   PH_CHECK_LAUNCH();
   return PH_OK;
@@ -285,13 +287,13 @@ extern "C" int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64
 extern "C" int ph_tets_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int64_t* tri_off,
                             const int32_t* tri_w, const int32_t* tri_fa, const int32_t* tri_fb,
                             const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
-                            const int64_t* tet_off, int32_t* tet_m, int32_t* tet_faces, int* d_status,
-                            void* stream) {
+                            const uint8_t* edge_enable, const int64_t* tet_off, int32_t* tet_m,
+                            int32_t* tet_faces, int* d_status, void* stream) {
   if (E <= 0) return E < 0 ? PH_ERR_ARG : PH_OK;
   ph::count_launch();
   k_tets<true><<<warp_grid(E), SX_NT, 0, (cudaStream_t)stream>>>(edge_i, edge_j, E, tri_off, tri_w, tri_fa,
-                                                                tri_fb, adj_ptr, adj_idx, adj_rank, nullptr,
-                                                                tet_off, tet_m, tet_faces, d_status);
+                                                                tri_fb, adj_ptr, adj_idx, adj_rank, edge_enable,
+                                                                nullptr, tet_off, tet_m, tet_faces, d_status);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

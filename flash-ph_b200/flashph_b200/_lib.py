@@ -47,8 +47,23 @@ _SIGS = {
     "ph_triangles_count": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, SZ, P]),
     "ph_triangles_emit": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, P, P, P]),
     "ph_tets_count_workspace_bytes": (SZ, [I64]),
-    "ph_tets_count": (ctypes.c_int, [P, P, I64, P, P, P, P, P, SZ, P]),
-    "ph_tets_emit": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, P, P, P, P, P, P]),
+    "ph_tets_count": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, SZ, P]),
+    "ph_tets_emit": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, P]),
+    "ph_cloud_tiles": (I64, [I64]),
+    "ph_batch_edges_enumerate": (ctypes.c_int, [P, P, I32, I64, P, P, P, I64, P, P]),
+    "ph_batch_vertex_cloud": (ctypes.c_int, [P, I32, P, P]),
+    "ph_batch_edges_sort_workspace_bytes": (SZ, [I64]),
+    "ph_batch_edges_sort": (ctypes.c_int, [P, P, P, I64, P, P, I32, I32, P, P, P, P, SZ, P]),
+    "ph_batch_item_offsets": (ctypes.c_int, [P, I64, P, I32, P, P]),
+    "ph_batch_h0_rows_workspace_bytes": (SZ, [I64]),
+    "ph_batch_h0_rows": (ctypes.c_int, [P, P, I64, P, P, I32, P, I64, P, P, SZ, P]),
+    "ph_batch_persistence_rows_workspace_bytes": (SZ, [I64]),
+    "ph_batch_persistence_rows": (ctypes.c_int, [P, P, I64, I32, P, P, P, P, I32, P, P, P, P, SZ, P]),
+    "ph_batch_edge_dim_mask": (ctypes.c_int, [P, I64, P, P, I32, P, P]),
+    "ph_or_gather_mask": (ctypes.c_int, [P, P, P, I64, I32, P]),
+    "ph_batch_knn_kth": (ctypes.c_int, [P, P, I32, P, I64, I32, I32, P, P]),
+    "ph_batch_quantile_workspace_bytes": (SZ, [I64]),
+    "ph_batch_quantile": (ctypes.c_int, [P, I64, P, P, I32, F64, P, P, SZ, P]),
     "ph_cofacet_csr_workspace_bytes": (SZ, [I64, I32]),
     "ph_cofacet_csr": (ctypes.c_int, [P, P, P, P, I32, I64, I64, I32, P, P, P, SZ, P]),
     "ph_cof_max_face": (ctypes.c_int, [P, P, P, P, I32, I64, I32, P, P, P]),

@@ -1,0 +1,392 @@
+"""Batching form: many point clouds of uneven n and d in one pipeline.
+
+A batch is the disjoint union of its clouds (vertex v of cloud c has global
+index vbase_c + v). Edge enumeration walks (cloud, 128x128 tile) work items
+from a segment table, the filtration sort orders every cloud's edges by its
+own packed key (local indices), and everything after it -- adjacency,
+forest, triangles, tetrahedra, cofacets, the lock-free reduction -- runs on
+global indices unchanged, because no simplex spans two clouds. Rows are cut
+per cloud at the end. Every cloud's diagrams equal those of a separate
+``rips_persistence`` call on it, bit for bit.
+
+Clouds are processed in chunks bounded by point and pair counts. Errors that
+the reference raises per call (validation, the triangle and tetrahedron
+caps) are returned per cloud as exception objects; they do not stop the
+batch.
+"""
+from __future__ import annotations
+
+import math
+from typing import Sequence
+
+import numpy as np
+import torch
+from torch import Tensor
+
+from . import _lib as L
+from .boruvka import boruvka_mask
+from .cohomology import Reduction, cof_max_face, cofacet_csr, reduce as _reduce
+from .rips import edge_filtration_values, threshold_sq, vertex_csr
+
+PH_ERR_POOL = 5
+SEG_DTYPE = np.dtype([("pt_off", "<i8"), ("vbase", "<i8"), ("tile_off", "<i8"), ("n", "<i4"), ("d", "<i4"),
+                      ("thr_sq", "<f4"), ("max_dim", "<i4")])
+assert SEG_DTYPE.itemsize == 40
+
+_CHUNK_POINTS = 1 << 18
+_CHUNK_PAIRS = 1 << 34
+
+
+def _validate(points, t, max_dim):
+    if t < 0:
+        return ValueError(f"max_edge_length must be non-negative, got {t}")
+    if points.ndim != 2:
+        return ValueError(f"points must have shape (n, d), got {tuple(points.shape)}")
+    if max_dim not in (0, 1, 2):
+        return ValueError(f"max_dim must be 0, 1, or 2, got {max_dim}")
+    if max_dim == 2 and points.shape[0] >= (1 << 16):
+        return ValueError(
+            f"H2 requires n < 65536 (16-bit vertex packing), got n={points.shape[0]}. "
+            f"Use max_dim=1 or reduce n.")
+    return None
+
+
+def _trivial(n, max_dim, device):
+    e = lambda: torch.empty(0, 2, dtype=torch.float32, device=device)  # noqa: E731
+    if n == 0:
+        return [e() for _ in range(max_dim + 1)]
+    h0 = torch.tensor([[0.0, float("inf")]], dtype=torch.float32, device=device)
+    return [h0] + [e() for _ in range(max_dim)]
+
+
+class _Batch:
+    """Device-side layout of one chunk of clouds."""
+
+    def __init__(self, pts_list, thrs, dims, device):
+        self.device = device
+        self.k = len(pts_list)
+        segs = np.zeros(self.k, dtype=SEG_DTYPE)
+        pt_off = vbase = tile_off = 0
+        for c, (p, t, md) in enumerate(zip(pts_list, thrs, dims)):
+            n, d = int(p.shape[0]), int(p.shape[1])
+            segs[c] = (pt_off, vbase, tile_off, n, d, threshold_sq(t), md)
+            pt_off += n * d
+            vbase += n
+            tile_off += int(L.query("ph_cloud_tiles", n))
+        self.segs_np = segs
+        self.N = vbase
+        self.ntiles = tile_off
+        self.max_dim = max(dims) if dims else 0
+        self.any_wrap = int(any(int(p.shape[0]) > 92682 for p in pts_list))
+        flat = [p.reshape(-1).float() for p in pts_list]
+        if not flat:
+            self.pts = torch.empty(0, device=device)
+        elif all(f.device.type == "cpu" for f in flat):
+            host = torch.cat(flat)
+            self.pts = host.pin_memory().to(device, non_blocking=True) if host.numel() else host.to(device)
+        else:
+            self.pts = torch.cat([f.to(device) for f in flat])
+        self.segs = torch.from_numpy(segs.view(np.uint8).copy()).to(device)
+        self.vcloud = torch.empty(max(self.N, 1), dtype=torch.int32, device=device)
+        L.call("ph_batch_vertex_cloud", self.segs.data_ptr(), self.k, self.vcloud.data_ptr(),
+               L.stream_handle(device))
+
+
+def _edges(b: _Batch):
+    dev = b.device
+    s = L.stream_handle(dev)
+    pairs = sum(int(n) * (int(n) - 1) // 2 for n in b.segs_np["n"])
+    cap = int(min(pairs, max(1 << 20, 64 * b.N)))
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    for _ in range(2):
+        cap = max(cap, 1)
+        ei = torch.empty(cap, dtype=torch.int32, device=dev)
+        ej = torch.empty(cap, dtype=torch.int32, device=dev)
+        ed = torch.empty(cap, dtype=torch.float32, device=dev)
+        L.call("ph_batch_edges_enumerate", b.pts.data_ptr(), b.segs.data_ptr(), b.k, b.ntiles, ei.data_ptr(),
+               ej.data_ptr(), ed.data_ptr(), cap, count.data_ptr(), s)
+        E = int(count.item())
+        if E <= cap:
+            break
+        if E >= 2 ** 31:
+            raise ValueError(f"Edge count {E} exceeds int32 range; reduce max_edge_length")
+        cap = E
+    ei, ej, ed = ei[:E], ej[:E], ed[:E]
+    oi, oj, od = torch.empty_like(ei), torch.empty_like(ej), torch.empty_like(ed)
+    if E:
+        nb = L.query("ph_batch_edges_sort_workspace_bytes", E)
+        ws = L.workspace(nb, dev)
+        L.call("ph_batch_edges_sort", ei.data_ptr(), ej.data_ptr(), ed.data_ptr(), E, b.vcloud.data_ptr(),
+               b.segs.data_ptr(), b.k, b.any_wrap, oi.data_ptr(), oj.data_ptr(), od.data_ptr(), ws.data_ptr(),
+               nb, s)
+    return oi, oj, od
+
+
+def _item_offsets(b: _Batch, item_vertex: Tensor):
+    off = torch.empty(b.k + 1, dtype=torch.int64, device=b.device)
+    L.call("ph_batch_item_offsets", L.ptr(item_vertex), item_vertex.numel(), b.vcloud.data_ptr(), b.k,
+           off.data_ptr(), L.stream_handle(b.device))
+    return off
+
+
+def _rows(red: Reduction, K: int, row_base: int, filt: Tensor, col_m, row_m, col_off: Tensor, nsegs: int):
+    dev = filt.device
+    rows = torch.empty(max(K, 1), 2, dtype=torch.float32, device=dev)
+    row_off = torch.empty(nsegs + 1, dtype=torch.int64, device=dev)
+    nrows = torch.zeros(1, dtype=torch.int64, device=dev)
+    nb = L.query("ph_batch_persistence_rows_workspace_bytes", K)
+    ws = L.workspace(nb, dev)
+    L.call("ph_batch_persistence_rows", L.ptr(red.state), L.ptr(red.piv), K, row_base, L.ptr(filt), L.ptr(col_m),
+           L.ptr(row_m), col_off.data_ptr(), nsegs, rows.data_ptr(), row_off.data_ptr(), nrows.data_ptr(),
+           ws.data_ptr(), nb, L.stream_handle(dev))
+    return rows, row_off
+
+
+class _Filt:
+    """RipsFiltration-shaped record for the shared stage functions."""
+
+    def __init__(self, ei, ej, ed, ptr, idx, rank):
+        self.edge_i, self.edge_j, self.edge_dist_sq = ei, ej, ed
+        self.vert_adj_ptr, self.vert_adj_idx, self.vert_adj_rank = ptr, idx, rank
+
+
+def _run_chunk(pts_list, thrs, dims, device, max_triangles, max_tetrahedra):
+    """Diagrams of every cloud of one chunk; raises _CapExceeded on caps."""
+    from .cohomology import enumerate_triangles
+
+    b = _Batch(pts_list, thrs, dims, device)
+    dev = device
+    s = L.stream_handle(dev)
+    ei, ej, ed = _edges(b)
+    E = ei.numel()
+    ptr, idx, rank = vertex_csr(ei, ej, b.N)
+    f = _Filt(ei, ej, ed, ptr, idx, rank)
+    filt = edge_filtration_values(ed)
+    mst, _, (_, mst_status) = boruvka_mask(ei, ej, b.N)
+    e_off = _item_offsets(b, ei)
+    h0 = torch.empty(max(b.N, 1), 2, dtype=torch.float32, device=dev)
+    nb = L.query("ph_batch_h0_rows_workspace_bytes", E)
+    ws = L.workspace(nb, dev)
+    L.call("ph_batch_h0_rows", L.ptr(filt), L.ptr(mst), E, e_off.data_ptr(), b.segs.data_ptr(), b.k,
+           b.vcloud.data_ptr(), b.N, h0.data_ptr(), ws.data_ptr(), nb, s)
+    out = {"h0": h0, "h0_off": torch.from_numpy(b.segs_np["vbase"].astype(np.int64))}
+    checks = [("ph_boruvka_mst", mst_status)]
+    if b.max_dim >= 1:
+        tris = enumerate_triangles(f, max_triangles=1 << 62)
+        T = tris.T
+        t_per_cloud = (tris.tri_off[e_off[1:]] - tris.tri_off[e_off[:-1]]).cpu().numpy()
+        over = [c for c in range(b.k) if dims[c] >= 1 and t_per_cloud[c] > max_triangles]
+        if over:
+            raise _CapExceeded({c: ValueError(
+                f"Triangle count {int(t_per_cloud[c])} exceeds max_triangles={max_triangles}. "
+                f"Reduce max_edge_length or increase max_triangles.") for c in over})
+        if T:
+            off1, data1 = cofacet_csr(E, E, T, 3, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb)
+        else:
+            off1 = torch.zeros(E + 1, dtype=torch.int32, device=dev)
+            data1 = torch.empty(0, dtype=torch.int32, device=dev)
+        # clouds that asked for H0 only get no H1 columns
+        skip1 = mst.clone()
+        if any(d < 1 for d in dims):
+            m1 = torch.empty(max(E, 1), dtype=torch.uint8, device=dev)
+            L.call("ph_batch_edge_dim_mask", L.ptr(ei), E, b.vcloud.data_ptr(), b.segs.data_ptr(), 1,
+                   m1.data_ptr(), s)
+            skip1 |= (m1[:E] == 0)
+        cmf1 = cof_max_face(T, 3, 0, mst, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb)
+        red1 = _reduce_retry(off1, data1, E, 0, T, E, skip1, cmf1, checks)
+        h1, h1_off = _rows(red1, E, E, filt, None, tris.tri_m, e_off, b.k)
+        out.update(h1=h1, h1_off=h1_off)
+        if b.max_dim >= 2:
+            en = torch.empty(max(E, 1), dtype=torch.uint8, device=dev)
+            L.call("ph_batch_edge_dim_mask", L.ptr(ei), E, b.vcloud.data_ptr(), b.segs.data_ptr(), 2,
+                   en.data_ptr(), s)
+            en = en[:E] if E else en
+            tet_off = torch.empty(E + 1, dtype=torch.int64, device=dev)
+            nb = L.query("ph_tets_count_workspace_bytes", E)
+            ws = L.workspace(nb, dev)
+            L.call("ph_tets_count", tris.tri_off.data_ptr(), L.ptr(tris.tri_w), E, ptr.data_ptr(), L.ptr(idx),
+                   L.ptr(rank), L.ptr(en), tet_off.data_ptr(), ws.data_ptr(), nb, s)
+            q_per_cloud = (tet_off[e_off[1:]] - tet_off[e_off[:-1]]).cpu().numpy()
+            over = [c for c in range(b.k) if dims[c] >= 2 and q_per_cloud[c] > max_tetrahedra]
+            if over:
+                raise _CapExceeded({c: ValueError(
+                    f"Tetrahedra count {int(q_per_cloud[c])} exceeds max_tetrahedra={max_tetrahedra}. "
+                    f"Reduce max_edge_length or increase max_tetrahedra.") for c in over})
+            Q = int(tet_off[E].item()) if E else 0
+            if E + T + Q >= 2 ** 31 or 4 * Q >= 2 ** 31:
+                raise ValueError(f"Tetrahedra count {Q} exceeds the int32 rank range")
+            tet_m = torch.empty(Q, dtype=torch.int32, device=dev)
+            tet_f = torch.empty(4 * Q, dtype=torch.int32, device=dev)
+            tstat = torch.zeros(1, dtype=torch.int32, device=dev)
+            if Q:
+                L.call("ph_tets_emit", L.ptr(ei), L.ptr(ej), E, tris.tri_off.data_ptr(), L.ptr(tris.tri_w),
+                       L.ptr(tris.tri_fa), L.ptr(tris.tri_fb), ptr.data_ptr(), L.ptr(idx), L.ptr(rank), L.ptr(en),
+                       tet_off.data_ptr(), tet_m.data_ptr(), tet_f.data_ptr(), tstat.data_ptr(), s)
+            skip2 = torch.empty(max(T, 1), dtype=torch.uint8, device=dev)
+            L.call("ph_mark_pivots", L.ptr(red1.state), L.ptr(red1.piv), E, E, skip2.data_ptr(), T, s)
+            if T:  # triangles of clouds without H2 are not columns
+                L.call("ph_or_gather_mask", skip2.data_ptr(), en.data_ptr(), tris.tri_m.data_ptr(), T, 1, s)
+            cmf2 = cof_max_face(Q, 4, E, skip2, faces_aos=tet_f)
+            if Q:
+                off2, data2 = cofacet_csr(T, E + T, Q, 4, faces_aos=tet_f)
+            else:
+                off2 = torch.zeros(T + 1, dtype=torch.int32, device=dev)
+                data2 = torch.empty(0, dtype=torch.int32, device=dev)
+            checks.append(("ph_tets_emit", tstat))
+            red2 = _reduce_retry(off2, data2, T, E, Q, E + T, skip2, cmf2, checks)
+            t_off = tris.tri_off[e_off].contiguous()
+            h2, h2_off = _rows(red2, T, E + T, filt, tris.tri_m, tet_m, t_off, b.k)
+            out.update(h2=h2, h2_off=h2_off)
+    # one host synchronisation for every status and offset
+    parts = [st.long().reshape(-1) for _, st in checks]
+    for key in ("h1_off", "h2_off"):
+        if key in out:
+            parts.append(out[key])
+    host = torch.cat(parts).cpu() if parts else torch.empty(0)
+    for k, (name, _) in enumerate(checks):
+        if int(host[k]) != 0:
+            raise L.PHError(name, int(host[k]))
+    pos = len(checks)
+    res = []
+    off_h = {}
+    for key in ("h1_off", "h2_off"):
+        if key in out:
+            off_h[key] = host[pos:pos + b.k + 1].tolist()
+            pos += b.k + 1
+    vb = b.segs_np["vbase"]
+    for c in range(b.k):
+        n = int(b.segs_np["n"][c])
+        dg = [out["h0"][int(vb[c]): int(vb[c]) + n]]
+        if dims[c] >= 1:
+            o = off_h["h1_off"]
+            dg.append(out["h1"][o[c]: o[c + 1]])
+        if dims[c] >= 2:
+            o = off_h["h2_off"]
+            dg.append(out["h2"][o[c]: o[c + 1]])
+        res.append(dg)
+    return res
+
+
+def _reduce_retry(off, data, K, col_base, R, row_base, skip, cmf, checks):
+    """Reduction whose status is read with the final synchronisation; a pool
+    overflow (rare) is detected here by a synchronous check and retried."""
+    nnz = int(data.numel())
+    pool_cap = max(4 * nnz, 1 << 20)
+    for _ in range(4):
+        red = _reduce(off, data, K, col_base, R, row_base, skip, cmf, pool_cap)
+        st = int(red.status.item())
+        if st == 0:
+            return red
+        if st != PH_ERR_POOL:
+            raise L.PHError("ph_reduce", st)
+        pool_cap *= 4
+    raise L.PHError("ph_reduce", PH_ERR_POOL, "pool still too small after retries")
+
+
+class _CapExceeded(Exception):
+    def __init__(self, errors: dict):
+        super().__init__("cap exceeded")
+        self.errors = errors
+
+
+def _chunks(order, sizes):
+    chunk, pts, pairs = [], 0, 0
+    for c in order:
+        n = sizes[c]
+        if chunk and (pts + n > _CHUNK_POINTS or pairs + n * n // 2 > _CHUNK_PAIRS):
+            yield chunk
+            chunk, pts, pairs = [], 0, 0
+        chunk.append(c)
+        pts += n
+        pairs += n * n // 2
+    if chunk:
+        yield chunk
+
+
+def rips_persistence_batch(
+    clouds: Sequence,
+    max_edge_lengths,
+    max_dim=1,
+    max_triangles: int = 10_000_000,
+    max_tetrahedra: int = 10_000_000,
+):
+    """Persistence diagrams of many point clouds.
+
+    Parameters
+    ----------
+    clouds : sequence of (n_c, d_c) arrays or tensors (n and d may differ).
+    max_edge_lengths : float or sequence of floats, one per cloud.
+    max_dim : int or sequence of ints (0, 1 or 2), one per cloud.
+    max_triangles, max_tetrahedra : per-cloud caps (the reference's defaults).
+
+    Returns
+    -------
+    list, one entry per cloud: the list of diagrams ``rips_persistence``
+    returns for that cloud (on the CUDA device), or the exception the
+    reference would raise for it.
+    """
+    k = len(clouds)
+    ts = [float(max_edge_lengths)] * k if np.isscalar(max_edge_lengths) else [float(x) for x in max_edge_lengths]
+    ds = [int(max_dim)] * k if np.isscalar(max_dim) else [int(x) for x in max_dim]
+    if len(ts) != k or len(ds) != k:
+        raise ValueError("one max_edge_length and one max_dim per cloud")
+    if not torch.cuda.is_available():
+        raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
+    device = torch.device("cuda", torch.cuda.current_device())
+    pts, results, todo = [], [None] * k, []
+    for c, p in enumerate(clouds):
+        t = p if isinstance(p, Tensor) else torch.from_numpy(np.ascontiguousarray(p))
+        err = _validate(t, ts[c], ds[c])
+        pts.append(t)
+        if err is not None:
+            results[c] = err
+        elif t.shape[0] <= 1:
+            results[c] = _trivial(t.shape[0], ds[c], device)
+        else:
+            todo.append(c)
+    sizes = {c: int(pts[c].shape[0]) for c in todo}
+    pending = list(todo)
+    while pending:
+        retry = []
+        for chunk in _chunks(pending, sizes):
+            try:
+                res = _run_chunk([pts[c].float().contiguous() for c in chunk], [ts[c] for c in chunk],
+                                 [ds[c] for c in chunk], device, max_triangles, max_tetrahedra)
+                for c, r in zip(chunk, res):
+                    results[c] = r
+            except _CapExceeded as ex:
+                for local, err in ex.errors.items():
+                    results[chunk[local]] = err
+                retry.extend(c for i, c in enumerate(chunk) if i not in ex.errors)
+        pending = retry
+    return results
+
+
+def auto_threshold_batch(clouds: Sequence, k: int = 20, percentile: float = 95.0) -> list[float]:
+    """``auto_threshold`` of every cloud (threshold.py:20-78), in one pass."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
+    device = torch.device("cuda", torch.cuda.current_device())
+    pts = [p if isinstance(p, Tensor) else torch.from_numpy(np.ascontiguousarray(p)) for p in clouds]
+    out = [0.0] * len(pts)
+    live = [c for c, p in enumerate(pts) if p.shape[0] > 1]
+    if not live:
+        return out
+    pct = max(0.0, min(100.0, percentile))
+    b = _Batch([pts[c].float().contiguous() for c in live], [0.0] * len(live), [0] * len(live), device)
+    qb = np.zeros(b.k + 1, dtype=np.int64)
+    qb[1:] = np.cumsum((b.segs_np["n"].astype(np.int64) + 127) // 128)
+    qb_dev = torch.from_numpy(qb).to(device)
+    kth = torch.empty(max(b.N, 1), dtype=torch.float32, device=device)
+    s = L.stream_handle(device)
+    L.call("ph_batch_knn_kth", b.pts.data_ptr(), b.segs.data_ptr(), b.k, qb_dev.data_ptr(), int(qb[-1]),
+           int(b.segs_np["d"].max()), max(1, k), kth.data_ptr(), s)
+    res = torch.empty(b.k, dtype=torch.float32, device=device)
+    nb = L.query("ph_batch_quantile_workspace_bytes", b.N)
+    ws = L.workspace(nb, device)
+    L.call("ph_batch_quantile", kth.data_ptr(), b.N, b.vcloud.data_ptr(), b.segs.data_ptr(), b.k, pct / 100.0,
+           res.data_ptr(), ws.data_ptr(), nb, s)
+    vals = res.cpu().tolist()
+    for c, v in zip(live, vals):
+        out[c] = float(v)
+    return out

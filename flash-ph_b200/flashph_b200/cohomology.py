@@ -157,7 +157,8 @@ def h1_diagram(filt, edge_filt: Tensor, mst_mask: Tensor, max_triangles: int = 1
     return rows, tris, red, info
 
 
-def h2_diagram(filt, edge_filt: Tensor, tris: Triangles, h1: Reduction, max_tetrahedra: int = 10_000_000):
+def h2_diagram(filt, edge_filt: Tensor, tris: Triangles, h1: Reduction, max_tetrahedra: int = 10_000_000,
+               edge_enable: Tensor | None = None):
     dev = edge_filt.device
     E = filt.edge_i.shape[0]
     T = tris.T
@@ -166,7 +167,8 @@ def h2_diagram(filt, edge_filt: Tensor, tris: Triangles, h1: Reduction, max_tetr
     nb = L.query("ph_tets_count_workspace_bytes", E)
     ws = L.workspace(nb, dev)
     L.call("ph_tets_count", tris.tri_off.data_ptr(), L.ptr(tris.tri_w), E, filt.vert_adj_ptr.data_ptr(),
-           L.ptr(filt.vert_adj_idx), L.ptr(filt.vert_adj_rank), tet_off.data_ptr(), ws.data_ptr(), nb, s)
+           L.ptr(filt.vert_adj_idx), L.ptr(filt.vert_adj_rank), L.ptr(edge_enable), tet_off.data_ptr(),
+           ws.data_ptr(), nb, s)
     Q = int(tet_off[E].item())
     if Q > max_tetrahedra:
         raise ValueError(
@@ -180,8 +182,8 @@ def h2_diagram(filt, edge_filt: Tensor, tris: Triangles, h1: Reduction, max_tetr
     if Q:
         L.call("ph_tets_emit", L.ptr(filt.edge_i), L.ptr(filt.edge_j), E, tris.tri_off.data_ptr(),
                L.ptr(tris.tri_w), L.ptr(tris.tri_fa), L.ptr(tris.tri_fb), filt.vert_adj_ptr.data_ptr(),
-               L.ptr(filt.vert_adj_idx), L.ptr(filt.vert_adj_rank), tet_off.data_ptr(), tet_m.data_ptr(),
-               tet_faces.data_ptr(), status.data_ptr(), s)
+               L.ptr(filt.vert_adj_idx), L.ptr(filt.vert_adj_rank), L.ptr(edge_enable), tet_off.data_ptr(),
+               tet_m.data_ptr(), tet_faces.data_ptr(), status.data_ptr(), s)
     skip2 = torch.empty(max(T, 1), dtype=torch.uint8, device=dev)
     L.call("ph_mark_pivots", L.ptr(h1.state), L.ptr(h1.piv), E, E, skip2.data_ptr(), T, s)
     cmf2 = cof_max_face(Q, 4, E, skip2, faces_aos=tet_faces)

@@ -45,6 +45,20 @@ unsigned long long ph_launch_count(void);
 
 /* ---- filtration -------------------------------------------------------- */
 
+/* One point cloud of a batch. A batch is the disjoint union of its clouds:
+ * cloud c's vertices get the global indices vbase .. vbase + n - 1, and all
+ * later stages (adjacency, forest, triangles, tetrahedra, reduction) work on
+ * global indices unchanged, since no simplex spans two clouds. */
+typedef struct ph_cloud_seg {
+  int64_t pt_off;   /* offset, in floats, of the cloud's first coordinate      */
+  int64_t vbase;    /* global index of the cloud's first vertex                */
+  int64_t tile_off; /* first edge-enumeration work item (ph_cloud_tiles each)  */
+  int32_t n;        /* points in the cloud                                      */
+  int32_t d;        /* dimension                                                */
+  float thr_sq;     /* fp32(max_edge_length^2)                                  */
+  int32_t max_dim;  /* 0, 1 or 2                                                */
+} ph_cloud_seg;
+
 /* All pairs i < j with sum_k (x_ik - x_jk)^2 < thr_sq, the squares
  * accumulated over k = 0..d-1 in order, one fused multiply-add per step,
  * in FP32. Replaces kernels/edge_kernel.py:152 direct_edge_enumerate (its
@@ -55,6 +69,16 @@ unsigned long long ph_launch_count(void);
 int ph_edges_enumerate(const float* pts, int64_t n, int32_t d, float thr_sq, int32_t* out_i,
                        int32_t* out_j, float* out_dsq, int64_t capacity,
                        unsigned long long* d_count, void* stream);
+
+/* Edge-enumeration work items (128 x 128 point tiles) of a cloud of n points. */
+int64_t ph_cloud_tiles(int64_t n);
+
+/* ph_edges_enumerate over a batch: segs (device) holds nsegs clouds ordered
+ * by tile_off; ntiles is the total number of work items. Vertex indices
+ * are written as global indices. */
+int ph_batch_edges_enumerate(const float* pts, const ph_cloud_seg* segs, int32_t nsegs, int64_t ntiles,
+                             int32_t* out_i, int32_t* out_j, float* out_dsq, int64_t capacity,
+                             unsigned long long* d_count, void* stream);
 
 /* Orders E edges by the reference's packed key
  *   (float bits of dist^2) << 32 | (j(j-1)/2 + i) & 0xFFFFFFFF
@@ -143,11 +167,14 @@ int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
  * p < q of third vertices of triangles with largest edge m such that (p,q)
  * is an edge ranked below m. Ordered by (largest edge rank, p, q).
  * Replaces triangle_kernel.py:402 tetrahedra_enumerate (count and emit
- * kernels, triangle_kernel.py:152-270). tet_off: E+1. */
+ * kernels, triangle_kernel.py:152-270). tet_off: E+1. edge_enable
+ * (optional, E bytes): only edges with a non-zero flag get tetrahedra (in a
+ * batch, the edges of clouds that asked for H2). */
 size_t ph_tets_count_workspace_bytes(int64_t E);
 int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64_t E,
                   const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
-                  int64_t* tet_off, void* workspace, size_t workspace_bytes, void* stream);
+                  const uint8_t* edge_enable, int64_t* tet_off, void* workspace,
+                  size_t workspace_bytes, void* stream);
 
 /* Writes per tetrahedron its largest edge and the local indices (triangle
  * global rank - E) of its four triangle faces. tet_faces: Q x 4.
@@ -156,8 +183,8 @@ int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64_t E,
 int ph_tets_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int64_t* tri_off,
                  const int32_t* tri_w, const int32_t* tri_fa, const int32_t* tri_fb,
                  const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
-                 const int64_t* tet_off, int32_t* tet_m, int32_t* tet_faces, int* d_status,
-                 void* stream);
+                 const uint8_t* edge_enable, const int64_t* tet_off, int32_t* tet_m,
+                 int32_t* tet_faces, int* d_status, void* stream);
 
 /* ---- coboundary columns and reduction ----------------------------------- */
 
@@ -212,13 +239,70 @@ int ph_mark_pivots(const int32_t* col_state, const int32_t* col_piv, int64_t K, 
 /* Persistence rows in the reference's order (reduce_h1_gpu.py:574-604):
  * apparent pairs by ascending column, then reduced pairs and essential
  * columns by descending column, pairs kept when death > birth (as float32),
- * then a stable sort by birth. Column c's value is filt[col_m ? col_m[c] : c],
+ * then a stable sort by birth. Columns in index order have non-decreasing
+ * birth values, so the sort only reorders runs of equal birth, which are
+ * ordered in place; no sort is run. Column c's value is filt[col_m ? col_m[c] : c],
  * row r's value is filt[row_m[r]]. out_rows: capacity K x 2; *d_nrows (int64). */
 size_t ph_persistence_rows_workspace_bytes(int64_t K);
 int ph_persistence_rows(const int32_t* col_state, const int32_t* col_piv, int64_t K,
                         int32_t row_base, const float* filt, const int32_t* col_m,
                         const int32_t* row_m, float* out_rows, int64_t* d_nrows, void* workspace,
                         size_t workspace_bytes, void* stream);
+
+/* ---- batches of clouds ---------------------------------------------------- */
+
+/* vcloud[v] = cloud of global vertex v (N = sum of n over the batch). */
+int ph_batch_vertex_cloud(const ph_cloud_seg* segs, int32_t nsegs, int32_t* vcloud, void* stream);
+
+/* Per-cloud filtration order of a batch's edges: each cloud's edges sorted
+ * by the reference's packed key computed with local vertex indices
+ * (rips.py:30-50), clouds in batch order. any_wrap != 0 when some cloud has
+ * n > 92682 (packed-key ties are then put in the reference's emission order). */
+size_t ph_batch_edges_sort_workspace_bytes(int64_t E);
+int ph_batch_edges_sort(const int32_t* in_i, const int32_t* in_j, const float* in_dsq, int64_t E,
+                        const int32_t* vcloud, const ph_cloud_seg* segs, int32_t nsegs, int32_t any_wrap,
+                        int32_t* out_i, int32_t* out_j, float* out_dsq, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* off[c] = first item of cloud c for items grouped by cloud, identified by
+ * one vertex each (item_vertex); off[nsegs] = n_items. */
+int ph_batch_item_offsets(const int32_t* item_vertex, int64_t n_items, const int32_t* vcloud, int32_t nsegs,
+                          int64_t* off, void* stream);
+
+/* H0 rows per cloud (persistence.py:169-192): cloud c's n rows start at row
+ * vbase_c. edge_off: per-cloud edge offsets. out_rows: N x 2. */
+size_t ph_batch_h0_rows_workspace_bytes(int64_t E);
+int ph_batch_h0_rows(const float* edge_filt, const uint8_t* mst_mask, int64_t E, const int64_t* edge_off,
+                     const ph_cloud_seg* segs, int32_t nsegs, const int32_t* vcloud, int64_t N,
+                     float* out_rows, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ph_persistence_rows per cloud: col_off (nsegs+1) are the per-cloud column
+ * offsets; row_off (nsegs+1) receives the per-cloud row offsets. */
+size_t ph_batch_persistence_rows_workspace_bytes(int64_t K);
+int ph_batch_persistence_rows(const int32_t* col_state, const int32_t* col_piv, int64_t K, int32_t row_base,
+                              const float* filt, const int32_t* col_m, const int32_t* row_m,
+                              const int64_t* col_off, int32_t nsegs, float* out_rows, int64_t* row_off,
+                              int64_t* d_nrows, void* workspace, size_t workspace_bytes, void* stream);
+
+/* out[e] = 1 if edge e's cloud has max_dim >= min_dim. */
+int ph_batch_edge_dim_mask(const int32_t* edge_i, int64_t E, const int32_t* vcloud, const ph_cloud_seg* segs,
+                           int32_t min_dim, uint8_t* out, void* stream);
+
+/* dst[i] |= src[idx[i]] (or its negation when invert != 0). */
+int ph_or_gather_mask(uint8_t* dst, const uint8_t* src, const int32_t* idx, int64_t n, int32_t invert,
+                      void* stream);
+
+/* k-th nearest-neighbour distance of every point of every cloud, k clamped
+ * to n_c - 1 per cloud. qb_off (nsegs+1): per-cloud offsets of 128-point
+ * query blocks; nqb their total; max_d the largest d. out: N floats. */
+int ph_batch_knn_kth(const float* pts, const ph_cloud_seg* segs, int32_t nsegs, const int64_t* qb_off,
+                     int64_t nqb, int32_t max_d, int32_t k, float* out, void* stream);
+
+/* torch.quantile semantics per cloud over values[vbase_c .. vbase_c+n_c). */
+size_t ph_batch_quantile_workspace_bytes(int64_t N);
+int ph_batch_quantile(const float* values, int64_t N, const int32_t* vcloud, const ph_cloud_seg* segs,
+                      int32_t nsegs, double q, float* out, void* workspace, size_t workspace_bytes,
+                      void* stream);
 
 /* ---- thresholds ---------------------------------------------------------- */
 

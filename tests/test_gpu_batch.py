@@ -1,0 +1,95 @@
+"""Batching form: a batch of clouds gives, per cloud, exactly the diagrams
+of separate rips_persistence calls (and of the oracle)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from golden_util import golden_cases, load_golden, sorted_rows
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.asarray(a, dtype=np.float32).view(np.uint32)
+
+
+def _same(a, b):
+    a = np.asarray(a.cpu() if isinstance(a, torch.Tensor) else a, dtype=np.float32).reshape(-1, 2)
+    b = np.asarray(b.cpu() if isinstance(b, torch.Tensor) else b, dtype=np.float32).reshape(-1, 2)
+    return a.shape == b.shape and np.array_equal(_bits(a), _bits(b))
+
+
+def test_batch_of_golden_clouds_equals_single_calls():
+    from flashph_b200 import rips_persistence
+    from flashph_b200.batch import rips_persistence_batch
+    names = golden_cases()
+    clouds, ts, dims = [], [], []
+    for nm in names:
+        z, meta = load_golden(nm)
+        clouds.append(z["points"])
+        ts.append(float(z["t"]))
+        dims.append(meta["max_dim"])
+    res = rips_persistence_batch(clouds, ts, dims)
+    assert len(res) == len(names)
+    for nm, p, t, md, r in zip(names, clouds, ts, dims, res):
+        assert not isinstance(r, Exception), (nm, r)
+        single = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=md)
+        assert len(r) == md + 1, nm
+        for dim in range(md + 1):
+            assert _same(r[dim], single[dim]), (nm, dim)
+
+
+def test_mixed_dims_and_sizes_against_oracle():
+    from flashph_b200.batch import rips_persistence_batch
+    rng = np.random.default_rng(11)
+    clouds, ts, dims = [], [], []
+    for c in range(24):
+        n = int(rng.integers(2, 400))
+        d = int(rng.choice([2, 3, 8, 32]))
+        clouds.append(rng.standard_normal((n, d)).astype(np.float32))
+        ts.append(float({2: 0.5, 3: 0.9, 8: 2.6, 32: 6.8}[d]))
+        dims.append(int(rng.choice([0, 1, 2])))
+    res = rips_persistence_batch(clouds, ts, dims)
+    for p, t, md, r in zip(clouds, ts, dims, res):
+        ref = oracle.run(p, t, md, fused=True)
+        assert _same(r[0], ref["h0"])
+        if md >= 1:
+            assert _same(r[1], ref["h1"])
+        if md >= 2:
+            assert _same(sorted_rows(r[2].cpu().numpy()), sorted_rows(ref["h2"]))
+
+
+def test_per_cloud_errors_do_not_stop_the_batch():
+    from flashph_b200.batch import rips_persistence_batch
+    rng = np.random.default_rng(3)
+    good = rng.standard_normal((50, 3)).astype(np.float32)
+    dense = rng.standard_normal((300, 3)).astype(np.float32) * 0.01
+    res = rips_persistence_batch([good, good, np.zeros((0, 3), np.float32), good[:1], dense],
+                                 [1.0, -1.0, 1.0, 1.0, 1.0], [1, 1, 2, 1, 1], max_triangles=100_000)
+    assert not isinstance(res[0], Exception)
+    assert isinstance(res[1], ValueError) and "non-negative" in str(res[1])
+    assert [x.shape for x in res[2]] == [(0, 2)] * 3
+    assert res[3][0].tolist() == [[0.0, float("inf")]]
+    assert isinstance(res[4], ValueError) and "max_triangles" in str(res[4])
+
+
+def test_auto_threshold_batch_equals_single():
+    from flashph_b200 import auto_threshold
+    from flashph_b200.batch import auto_threshold_batch
+    rng = np.random.default_rng(5)
+    clouds = [rng.standard_normal((int(n), int(d))).astype(np.float32)
+              for n, d in zip(rng.integers(2, 700, 12), rng.choice([3, 8, 32], 12))]
+    clouds.append(np.zeros((1, 3), np.float32))
+    got = auto_threshold_batch(clouds, k=20, percentile=95.0)
+    want = [auto_threshold(torch.from_numpy(c).cuda(), k=20, percentile=95.0) for c in clouds]
+    assert got == want
+    # and within float32 rounding of a float64 restatement
+    for c, g in zip(clouds[:-1], got[:-1]):
+        d2 = ((c[:, None, :].astype(np.float64) - c[None, :, :]) ** 2).sum(-1)
+        np.fill_diagonal(d2, np.inf)
+        k = max(1, min(20, c.shape[0] - 1))
+        kth = np.sqrt(np.sort(d2, axis=1)[:, k - 1])
+        assert abs(g - np.quantile(kth, 0.95)) <= 1e-5 * max(1.0, abs(g))
