@@ -5,6 +5,16 @@ max_edge_length=1.4, max_dim=2 (the reference's "20K x 10 H0-H2 ms"
 figure). Synthetic data. One step = one full rips_persistence call.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {flashph,reference}]
+                  [--workload {plain,batch,serve}]
+
+The default line also carries a ``serving`` block: a seeded sample of the
+serving request stream (n log-uniform in [100, 50000], d in {4, 10, 50},
+threshold = 95th percentile of 20-NN distances, H2 for 20% of requests)
+served by the continuous-batching server and by plain per-call
+rips_persistence: throughput with every request queued at once, and p50/p99
+latency under Poisson arrivals at half the plain path's capacity.
+``--workload batch`` runs the batching configuration (4096 clouds);
+``--workload serve`` runs the serving stream over a rate sweep.
 
 Prints one JSON line on rank 0. ``value`` is the device-timed ms per call
 with the points resident in HBM; ``e2e`` is the same call made through the
@@ -106,6 +116,181 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ---- serving and batching workloads ------------------------------------------------
+def serving_requests(count, seed=7):
+    """Seeded sample of the serving stream: n log-uniform in [100, 50000],
+    d in {4, 10, 50}, i.i.d. N(0,1) float32, H2 for 20% of requests."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(count):
+        n = int(np.exp(rng.uniform(np.log(100), np.log(50000))))
+        d = int(rng.choice([4, 10, 50]))
+        md = 2 if rng.random() < 0.2 else 1
+        reqs.append([rng.standard_normal((n, d)).astype(np.float32), None, md])
+    return reqs
+
+
+def clifford_cloud(n, d, rng):
+    th = rng.uniform(0, 2 * np.pi, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    p = np.column_stack([np.cos(th), np.sin(th), np.cos(ph), np.sin(ph)]) / np.sqrt(2)
+    p = p + rng.standard_normal((n, 4)) * 0.02
+    full = np.zeros((n, max(d, 4)))
+    full[:, :4] = p
+    q, r = np.linalg.qr(rng.standard_normal((full.shape[1], full.shape[1])))
+    q = q * np.sign(np.diag(r))
+    return (full @ q.T)[:, :d].astype(np.float32)
+
+
+def batching_clouds(count, seed=11):
+    """Seeded batching configuration: n log-uniform in [64, 4096], d in
+    {3, 8, 32}; even clouds i.i.d. N(0,1), odd clouds noisy Clifford tori
+    rotated by a random orthogonal matrix (for d = 3 the first three rotated
+    coordinates of the 4-D torus are kept)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(count):
+        n = int(np.exp(rng.uniform(np.log(64), np.log(4096))))
+        d = int(rng.choice([3, 8, 32]))
+        out.append(rng.standard_normal((n, d)).astype(np.float32) if c % 2 == 0 else clifford_cloud(n, d, rng))
+    return out
+
+
+def _thresholds(clouds):
+    from flashph_b200.batch import auto_threshold_batch
+    return auto_threshold_batch(clouds, k=20, percentile=95.0)
+
+
+def _plain_stream(reqs, arrivals):
+    import torch
+    from flashph_b200 import rips_persistence
+    t0 = time.perf_counter()
+    done, ok = [], 0
+    for (p, t, md), a in zip(reqs, arrivals):
+        wait = t0 + a - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        try:
+            rips_persistence(p, t, max_dim=md)
+            ok += 1
+        except ValueError:
+            pass
+        torch.cuda.synchronize()
+        done.append(time.perf_counter() - t0)
+    return np.asarray(done), ok
+
+
+def _served_stream(reqs, arrivals, slots=2):
+    from flashph_b200.serve import PersistenceServer
+    t0 = time.perf_counter()
+    done = [0.0] * len(reqs)
+    futs = []
+    with PersistenceServer(slots=slots) as srv:
+        for k, ((p, t, md), a) in enumerate(zip(reqs, arrivals)):
+            wait = t0 + a - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            f = srv.submit(p, t, md)
+            f.add_done_callback(lambda _f, k=k: done.__setitem__(k, time.perf_counter() - t0))
+            futs.append(f)
+        ok = 0
+        for f in futs:
+            try:
+                f.result(timeout=600)
+                ok += 1
+            except ValueError:
+                pass
+        batches = srv.batches
+    return np.asarray(done), ok, batches
+
+
+def serving_summary(count, rates_rel=(0.5,), seed=7):
+    """Throughput (all requests queued at once) and latency at Poisson rates
+    given relative to the plain path's measured capacity."""
+    reqs = serving_requests(count, seed)
+    thr = _thresholds([r[0] for r in reqs])
+    for r, t in zip(reqs, thr):
+        r[1] = t
+    # warm both paths
+    _plain_stream(reqs[:4], np.zeros(4))
+    _served_stream(reqs[:4], np.zeros(4))
+    burst = np.zeros(count)
+    pd, pok = _plain_stream(reqs, burst)
+    sd, sok, nb = _served_stream(reqs, burst)
+    plain_rate = count / pd.max()
+    served_rate = count / sd.max()
+    out = {"requests": count, "ok": int(sok), "plain_ok": int(pok), "capped_or_invalid": int(count - sok),
+           "plain_diagrams_per_s": round(plain_rate, 2), "served_diagrams_per_s": round(served_rate, 2),
+           "served_over_plain": round(served_rate / plain_rate, 3), "served_batches_burst": int(nb),
+           "rates": []}
+    rng = np.random.default_rng(seed + 1)
+    for rel in rates_rel:
+        lam = rel * plain_rate
+        arr = np.cumsum(rng.exponential(1.0 / lam, count))
+        pd, _ = _plain_stream(reqs, arr)
+        sd, _, nb = _served_stream(reqs, arr)
+        pl, sl = (pd - arr) * 1e3, (sd - arr) * 1e3
+        out["rates"].append({"rate_per_s": round(lam, 2), "rate_rel_plain_capacity": rel,
+                             "plain_p50_ms": round(float(np.percentile(pl, 50)), 3),
+                             "plain_p99_ms": round(float(np.percentile(pl, 99)), 3),
+                             "served_p50_ms": round(float(np.percentile(sl, 50)), 3),
+                             "served_p99_ms": round(float(np.percentile(sl, 99)), 3),
+                             "served_batches": int(nb)})
+    return out
+
+
+def run_batching(args, rank, local):
+    """Batching configuration: diagrams/s of one batched call over every
+    cloud against plain per-call rips_persistence on a prefix of them."""
+    import torch
+    from flashph_b200 import rips_persistence
+    from flashph_b200.batch import rips_persistence_batch
+
+    torch.cuda.set_device(local)
+    clouds = batching_clouds(args.clouds)
+    thr = _thresholds(clouds)
+    rips_persistence_batch(clouds[:8], thr[:8], 1)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = rips_persistence_batch(clouds, thr, 1)
+    torch.cuda.synchronize()
+    bt = time.perf_counter() - t0
+    ok = sum(not isinstance(r, Exception) for r in res)
+    m = min(len(clouds), max(64, args.clouds // 8))
+    t0 = time.perf_counter()
+    pok = 0
+    for p, t in zip(clouds[:m], thr[:m]):
+        try:
+            rips_persistence(p, t, max_dim=1)
+            pok += 1
+        except ValueError:
+            pass
+    torch.cuda.synchronize()
+    pt = time.perf_counter() - t0
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched diagrams/s", "value": round(len(clouds) / bt, 2), "unit": "diagrams/s",
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "batching: n log-uniform [64,4096], d in {3,8,32}, half N(0,1), half "
+                                   "rotated noisy Clifford tori, t = 95th pct 20-NN, max_dim=1",
+                       "clouds": len(clouds), "ok": ok, "capped": len(clouds) - ok},
+            "batch_seconds": round(bt, 3),
+            "plain_per_call": {"clouds": m, "seconds": round(pt, 3), "ok": pok,
+                               "diagrams_per_s": round(m / pt, 2)},
+            "batched_over_plain": round((len(clouds) / bt) / (m / pt), 3)}), flush=True)
+
+
+def run_serving(args, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    out = serving_summary(args.serving_requests, rates_rel=(0.25, 0.5, 1.0, 2.0))
+    if rank == 0:
+        print(json.dumps({"metric": "served diagrams/s", "value": out["served_diagrams_per_s"],
+                          "unit": "diagrams/s", "higher_is_better": True, "data": "synthetic", "dtype": "f32",
+                          "config": {"workload": "serving: n log-uniform [100,50000], d in {4,10,50}, N(0,1), "
+                                                 "t = 95th pct 20-NN, H2 for 20%"}, "serving": out}), flush=True)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -152,10 +337,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("flashph", "reference"), default="flashph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=96)
+    ap.add_argument("--workload", choices=("plain", "batch", "serve"), default="plain")
+    ap.add_argument("--clouds", type=int, default=4096)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "batch":
+        run_batching(args, rank, local)
+        return
+    if args.workload == "serve":
+        run_serving(args, rank, local)
         return
 
     import torch
@@ -263,6 +458,8 @@ def main():
             "cpu_baseline": cpu,
             "clocks": cs,
         }
+        if not args.no_serving:
+            line["serving"] = serving_summary(args.serving_requests, rates_rel=(0.5,))
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

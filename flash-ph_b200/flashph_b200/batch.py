@@ -35,6 +35,8 @@ assert SEG_DTYPE.itemsize == 40
 
 _CHUNK_POINTS = 1 << 18
 _CHUNK_PAIRS = 1 << 34
+_CHUNK_TRIANGLES = 1 << 28   # per chunk, keeps every global rank in int32
+_CHUNK_TETS = 1 << 28
 
 
 def _validate(points, t, max_dim):
@@ -96,7 +98,7 @@ def _edges(b: _Batch):
     dev = b.device
     s = L.stream_handle(dev)
     pairs = sum(int(n) * (int(n) - 1) // 2 for n in b.segs_np["n"])
-    cap = int(min(pairs, max(1 << 20, 64 * b.N)))
+    cap = int(min(pairs, max(1 << 20, 256 * b.N)))
     count = torch.zeros(1, dtype=torch.int64, device=dev)
     for _ in range(2):
         cap = max(cap, 1)
@@ -152,7 +154,7 @@ class _Filt:
 
 def _run_chunk(pts_list, thrs, dims, device, max_triangles, max_tetrahedra):
     """Diagrams of every cloud of one chunk; raises _CapExceeded on caps."""
-    from .cohomology import enumerate_triangles
+    from .cohomology import count_triangles, emit_triangles
 
     b = _Batch(pts_list, thrs, dims, device)
     dev = device
@@ -172,14 +174,17 @@ def _run_chunk(pts_list, thrs, dims, device, max_triangles, max_tetrahedra):
     out = {"h0": h0, "h0_off": torch.from_numpy(b.segs_np["vbase"].astype(np.int64))}
     checks = [("ph_boruvka_mst", mst_status)]
     if b.max_dim >= 1:
-        tris = enumerate_triangles(f, max_triangles=1 << 62)
-        T = tris.T
-        t_per_cloud = (tris.tri_off[e_off[1:]] - tris.tri_off[e_off[:-1]]).cpu().numpy()
+        tri_off = count_triangles(f)
+        t_per_cloud = (tri_off[e_off[1:]] - tri_off[e_off[:-1]]).cpu().numpy()
         over = [c for c in range(b.k) if dims[c] >= 1 and t_per_cloud[c] > max_triangles]
         if over:
             raise _CapExceeded({c: ValueError(
                 f"Triangle count {int(t_per_cloud[c])} exceeds max_triangles={max_triangles}. "
                 f"Reduce max_edge_length or increase max_triangles.") for c in over})
+        T = int(t_per_cloud.sum())
+        if E + 3 * T >= 2 ** 31 or T > _CHUNK_TRIANGLES:
+            raise _ChunkTooBig()
+        tris = emit_triangles(f, tri_off, T)
         if T:
             off1, data1 = cofacet_csr(E, E, T, 3, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb)
         else:
@@ -212,9 +217,9 @@ def _run_chunk(pts_list, thrs, dims, device, max_triangles, max_tetrahedra):
                 raise _CapExceeded({c: ValueError(
                     f"Tetrahedra count {int(q_per_cloud[c])} exceeds max_tetrahedra={max_tetrahedra}. "
                     f"Reduce max_edge_length or increase max_tetrahedra.") for c in over})
-            Q = int(tet_off[E].item()) if E else 0
-            if E + T + Q >= 2 ** 31 or 4 * Q >= 2 ** 31:
-                raise ValueError(f"Tetrahedra count {Q} exceeds the int32 rank range")
+            Q = int(q_per_cloud.sum())
+            if E + T + Q >= 2 ** 31 or 4 * Q >= 2 ** 31 or Q > _CHUNK_TETS:
+                raise _ChunkTooBig()
             tet_m = torch.empty(Q, dtype=torch.int32, device=dev)
             tet_f = torch.empty(4 * Q, dtype=torch.int32, device=dev)
             tstat = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -283,6 +288,10 @@ def _reduce_retry(off, data, K, col_base, R, row_base, skip, cmf, checks):
     raise L.PHError("ph_reduce", PH_ERR_POOL, "pool still too small after retries")
 
 
+class _ChunkTooBig(Exception):
+    """The chunk's simplices do not fit the rank range or the memory budget."""
+
+
 class _CapExceeded(Exception):
     def __init__(self, errors: dict):
         super().__init__("cap exceeded")
@@ -345,20 +354,26 @@ def rips_persistence_batch(
         else:
             todo.append(c)
     sizes = {c: int(pts[c].shape[0]) for c in todo}
-    pending = list(todo)
-    while pending:
-        retry = []
-        for chunk in _chunks(pending, sizes):
-            try:
-                res = _run_chunk([pts[c].float().contiguous() for c in chunk], [ts[c] for c in chunk],
-                                 [ds[c] for c in chunk], device, max_triangles, max_tetrahedra)
-                for c, r in zip(chunk, res):
-                    results[c] = r
-            except _CapExceeded as ex:
-                for local, err in ex.errors.items():
-                    results[chunk[local]] = err
-                retry.extend(c for i, c in enumerate(chunk) if i not in ex.errors)
-        pending = retry
+    work = list(_chunks(todo, sizes))
+    while work:
+        chunk = work.pop(0)
+        try:
+            res = _run_chunk([pts[c].float().contiguous() for c in chunk], [ts[c] for c in chunk],
+                             [ds[c] for c in chunk], device, max_triangles, max_tetrahedra)
+            for c, r in zip(chunk, res):
+                results[c] = r
+        except _CapExceeded as ex:
+            for local, err in ex.errors.items():
+                results[chunk[local]] = err
+            rest = [c for i, c in enumerate(chunk) if i not in ex.errors]
+            if rest:
+                work.insert(0, rest)
+        except _ChunkTooBig:
+            if len(chunk) == 1:
+                results[chunk[0]] = ValueError("Simplex count exceeds the int32 rank range")
+            else:
+                h = len(chunk) // 2
+                work[:0] = [chunk[:h], chunk[h:]]
     return results
 
 

@@ -40,24 +40,23 @@ class Reduction(NamedTuple):
     status: Tensor  # (1,) int32 device status
 
 
-def enumerate_triangles(filt, max_triangles: int = 10_000_000) -> Triangles:
+def count_triangles(filt) -> Tensor:
+    """tri_off (E+1, int64): triangles grouped by largest edge (no host sync)."""
     dev = filt.edge_i.device
     E = filt.edge_i.shape[0]
-    s = L.stream_handle(dev)
     tri_off = torch.empty(E + 1, dtype=torch.int64, device=dev)
     cof_off = torch.empty(E + 1, dtype=torch.int64, device=dev)
     nb = L.query("ph_triangles_count_workspace_bytes", E)
     ws = L.workspace(nb, dev)
     L.call("ph_triangles_count", L.ptr(filt.edge_i), L.ptr(filt.edge_j), E, filt.vert_adj_ptr.data_ptr(),
            L.ptr(filt.vert_adj_idx), L.ptr(filt.vert_adj_rank), tri_off.data_ptr(), cof_off.data_ptr(),
-           ws.data_ptr(), nb, s)
-    T = int(tri_off[E].item())
-    if T > max_triangles:
-        raise ValueError(
-            f"Triangle count {T} exceeds max_triangles={max_triangles}. "
-            f"Reduce max_edge_length or increase max_triangles.")
-    if E + 3 * T >= 2 ** 31:
-        raise ValueError(f"Triangle count {T} exceeds the int32 rank range")
+           ws.data_ptr(), nb, L.stream_handle(dev))
+    return tri_off
+
+
+def emit_triangles(filt, tri_off: Tensor, T: int) -> Triangles:
+    dev = filt.edge_i.device
+    E = filt.edge_i.shape[0]
     tm = torch.empty(T, dtype=torch.int32, device=dev)
     tw = torch.empty(T, dtype=torch.int32, device=dev)
     tfa = torch.empty(T, dtype=torch.int32, device=dev)
@@ -65,8 +64,21 @@ def enumerate_triangles(filt, max_triangles: int = 10_000_000) -> Triangles:
     if T:
         L.call("ph_triangles_emit", L.ptr(filt.edge_i), L.ptr(filt.edge_j), E, filt.vert_adj_ptr.data_ptr(),
                L.ptr(filt.vert_adj_idx), L.ptr(filt.vert_adj_rank), tri_off.data_ptr(), tm.data_ptr(),
-               tw.data_ptr(), tfa.data_ptr(), tfb.data_ptr(), s)
+               tw.data_ptr(), tfa.data_ptr(), tfb.data_ptr(), L.stream_handle(dev))
     return Triangles(T, tri_off, tm, tw, tfa, tfb)
+
+
+def enumerate_triangles(filt, max_triangles: int = 10_000_000) -> Triangles:
+    E = filt.edge_i.shape[0]
+    tri_off = count_triangles(filt)
+    T = int(tri_off[E].item())
+    if T > max_triangles:
+        raise ValueError(
+            f"Triangle count {T} exceeds max_triangles={max_triangles}. "
+            f"Reduce max_edge_length or increase max_triangles.")
+    if E + 3 * T >= 2 ** 31:
+        raise ValueError(f"Triangle count {T} exceeds the int32 rank range")
+    return emit_triangles(filt, tri_off, T)
 
 
 def cofacet_csr(n_faces: int, row_base: int, S: int, k: int, faces_aos=None, f0=None, f1=None, f2=None):

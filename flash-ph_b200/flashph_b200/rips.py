@@ -46,7 +46,7 @@ def enumerate_edges(points: Tensor, max_edge_length: float):
     thr = threshold_sq(max_edge_length)
     s = L.stream_handle(dev)
     pairs = n * (n - 1) // 2
-    cap = int(min(pairs, max(_MIN_EDGE_CAPACITY, 32 * n)))
+    cap = int(min(pairs, max(_MIN_EDGE_CAPACITY, 256 * n)))
     count = torch.zeros(1, dtype=torch.int64, device=dev)
     for _ in range(2):
         cap = max(cap, 1)

@@ -1,0 +1,138 @@
+"""Serving form: a continuous-batching request loop on one GPU.
+
+``PersistenceServer.submit(points, max_edge_length, max_dim)`` returns a
+future. Worker slots (one CUDA stream each) take every queued request that
+fits the admission limits, run them as one batch through the batching
+pipeline (``batch.rips_persistence_batch``) and resolve the futures; while
+one slot's batch is on the device, the next slot admits the requests that
+arrived in the meantime, so batches overlap on the GPU. Admission is by
+memory, estimated from the request sizes (points, candidate pairs); the
+pipeline's own counting pass then enforces the reference's per-call
+triangle and tetrahedron caps per request.
+
+Every result equals what ``rips_persistence`` returns for that request
+alone, bit for bit: requests never interact inside a batch.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+import torch
+
+from .batch import rips_persistence_batch
+
+
+class _Request:
+    __slots__ = ("points", "t", "max_dim", "future", "arrival", "done", "n")
+
+    def __init__(self, points, t, max_dim):
+        self.points = points
+        self.t = float(t)
+        self.max_dim = int(max_dim)
+        self.future: Future = Future()
+        self.arrival = time.perf_counter()
+        self.done = None
+        self.n = int(points.shape[0]) if hasattr(points, "shape") and len(points.shape) else 0
+
+
+class PersistenceServer:
+    """Continuous batching of ``rips_persistence`` requests.
+
+    Parameters
+    ----------
+    slots : concurrent batches in flight (each on its own stream).
+    max_batch_points : admission limit on the points of one batch.
+    max_batch_pairs : admission limit on candidate point pairs of one batch.
+    max_batch_requests : admission limit on requests per batch.
+    """
+
+    def __init__(self, device=None, slots: int = 2, max_batch_points: int = 1 << 17,
+                 max_batch_pairs: int = 1 << 32, max_batch_requests: int = 1024,
+                 max_triangles: int = 10_000_000, max_tetrahedra: int = 10_000_000):
+        if not torch.cuda.is_available():
+            raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.max_batch_points = max_batch_points
+        self.max_batch_pairs = max_batch_pairs
+        self.max_batch_requests = max_batch_requests
+        self.max_triangles = max_triangles
+        self.max_tetrahedra = max_tetrahedra
+        self._queue: collections.deque[_Request] = collections.deque()
+        self._cv = threading.Condition()
+        self._closed = False
+        self.batches = 0
+        self._workers = [threading.Thread(target=self._worker, daemon=True, name=f"ph-slot-{i}")
+                         for i in range(slots)]
+        for w in self._workers:
+            w.start()
+
+    def submit(self, points, max_edge_length: float, max_dim: int = 1) -> Future:
+        """Queue one request; the future resolves to the list of diagrams."""
+        req = _Request(points, max_edge_length, max_dim)
+        with self._cv:
+            if self._closed:
+                raise RuntimeError("server is closed")
+            self._queue.append(req)
+            self._cv.notify()
+        return req.future
+
+    def close(self):
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        for w in self._workers:
+            w.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _admit(self) -> list[_Request]:
+        batch, pts, pairs = [], 0, 0
+        while self._queue and len(batch) < self.max_batch_requests:
+            r = self._queue[0]
+            n = r.n
+            if batch and (pts + n > self.max_batch_points or pairs + n * n // 2 > self.max_batch_pairs):
+                break
+            batch.append(self._queue.popleft())
+            pts += n
+            pairs += n * n // 2
+        return batch
+
+    def _worker(self):
+        torch.cuda.set_device(self.device)
+        stream = torch.cuda.Stream(self.device)
+        while True:
+            with self._cv:
+                while not self._queue and not self._closed:
+                    self._cv.wait()
+                if not self._queue and self._closed:
+                    return
+                batch = self._admit()
+            try:
+                with torch.cuda.stream(stream):
+                    res = rips_persistence_batch([r.points for r in batch], [r.t for r in batch],
+                                                 [r.max_dim for r in batch], self.max_triangles,
+                                                 self.max_tetrahedra)
+                stream.synchronize()
+                self.batches += 1
+            except Exception as ex:  # a failure of the whole batch goes to each request
+                res = [ex] * len(batch)
+            now = time.perf_counter()
+            for r, out in zip(batch, res):
+                r.done = now
+                if isinstance(out, Exception):
+                    r.future.set_exception(out)
+                else:
+                    r.future.set_result(out)
+
+
+def latency_percentiles(arrivals, completions, qs=(50, 99)):
+    lat = (np.asarray(completions) - np.asarray(arrivals)) * 1e3
+    return {f"p{q}": float(np.percentile(lat, q)) for q in qs}
