@@ -50,6 +50,9 @@ _SIGS = {
     "ph_tets_count": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, SZ, P]),
     "ph_tets_emit": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, P]),
     "ph_cloud_tiles": (I64, [I64]),
+    "ph_edges_screened_workspace_bytes": (SZ, [I64, I32, I32]),
+    "ph_batch_edges_enumerate_screened": (ctypes.c_int, [P, P, I32, I64, I32, I64, P, I64, P, P, P, I64, P, P, P,
+                                                         P, SZ, P]),
     "ph_batch_edges_enumerate": (ctypes.c_int, [P, P, I32, I64, P, P, P, I64, P, P]),
     "ph_batch_vertex_cloud": (ctypes.c_int, [P, I32, P, P]),
     "ph_batch_edges_sort_workspace_bytes": (SZ, [I64]),

@@ -95,25 +95,14 @@ class _Batch:
 
 
 def _edges(b: _Batch):
+    from ._edges import enumerate_segments
+
     dev = b.device
     s = L.stream_handle(dev)
     pairs = sum(int(n) * (int(n) - 1) // 2 for n in b.segs_np["n"])
     cap = int(min(pairs, max(1 << 20, 256 * b.N)))
-    count = torch.zeros(1, dtype=torch.int64, device=dev)
-    for _ in range(2):
-        cap = max(cap, 1)
-        ei = torch.empty(cap, dtype=torch.int32, device=dev)
-        ej = torch.empty(cap, dtype=torch.int32, device=dev)
-        ed = torch.empty(cap, dtype=torch.float32, device=dev)
-        L.call("ph_batch_edges_enumerate", b.pts.data_ptr(), b.segs.data_ptr(), b.k, b.ntiles, ei.data_ptr(),
-               ej.data_ptr(), ed.data_ptr(), cap, count.data_ptr(), s)
-        E = int(count.item())
-        if E <= cap:
-            break
-        if E >= 2 ** 31:
-            raise ValueError(f"Edge count {E} exceeds int32 range; reduce max_edge_length")
-        cap = E
-    ei, ej, ed = ei[:E], ej[:E], ed[:E]
+    ei, ej, ed = enumerate_segments(b.pts, b.segs_np, b.segs, b.ntiles, cap)
+    E = ei.numel()
     oi, oj, od = torch.empty_like(ei), torch.empty_like(ej), torch.empty_like(ed)
     if E:
         nb = L.query("ph_batch_edges_sort_workspace_bytes", E)

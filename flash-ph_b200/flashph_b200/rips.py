@@ -20,6 +20,9 @@ from . import _timing
 # Initial edge-buffer capacity; a run with more edges is repeated once with
 # the exact count.
 _MIN_EDGE_CAPACITY = 1 << 22
+# ph_cloud_seg (include/flashph_b200.h)
+_SEG_DTYPE = np.dtype([("pt_off", "<i8"), ("vbase", "<i8"), ("tile_off", "<i8"), ("n", "<i4"), ("d", "<i4"),
+                       ("thr_sq", "<f4"), ("max_dim", "<i4")])
 
 
 class RipsFiltration(NamedTuple):
@@ -35,34 +38,27 @@ class RipsFiltration(NamedTuple):
 
 
 def threshold_sq(max_edge_length: float) -> float:
-    """fp32 of the double product t*t, as the reference's kernel argument."""
-    return float(np.float32(float(max_edge_length) * float(max_edge_length)))
+    """fp32 of the double product t*t, as the reference's kernel argument
+    (inf when the product exceeds the fp32 range)."""
+    with np.errstate(over="ignore"):
+        return float(np.float32(float(max_edge_length) * float(max_edge_length)))
 
 
-def enumerate_edges(points: Tensor, max_edge_length: float):
-    """Unsorted edges (i, j, dist^2) of all pairs with dist^2 < fp32(t*t)."""
+def enumerate_edges(points: Tensor, max_edge_length: float, screen: bool | None = None, stats: bool = False):
+    """Unsorted edges (i, j, dist^2) of all pairs with dist^2 < fp32(t*t).
+
+    ``screen`` forces the tensor-core screened kernel (True) or the direct
+    kernel (False); None picks by dimension. Both give the same edges."""
+    from ._edges import enumerate_segments
+
     dev = points.device
     n, d = points.shape
-    thr = threshold_sq(max_edge_length)
-    s = L.stream_handle(dev)
+    seg = np.zeros(1, dtype=_SEG_DTYPE)
+    seg[0] = (0, 0, 0, n, d, threshold_sq(max_edge_length), 1)
+    seg_dev = torch.from_numpy(seg.view(np.uint8).copy()).to(dev, non_blocking=True)
     pairs = n * (n - 1) // 2
     cap = int(min(pairs, max(_MIN_EDGE_CAPACITY, 256 * n)))
-    count = torch.zeros(1, dtype=torch.int64, device=dev)
-    for _ in range(2):
-        cap = max(cap, 1)
-        ei = torch.empty(cap, dtype=torch.int32, device=dev)
-        ej = torch.empty(cap, dtype=torch.int32, device=dev)
-        ed = torch.empty(cap, dtype=torch.float32, device=dev)
-        with _timing.stage("edges"):
-            L.call("ph_edges_enumerate", points.data_ptr(), n, d, thr, ei.data_ptr(), ej.data_ptr(),
-                   ed.data_ptr(), cap, count.data_ptr(), s)
-        E = int(count.item())
-        if E <= cap:
-            return ei[:E], ej[:E], ed[:E]
-        if E >= 2 ** 31:
-            raise ValueError(f"Edge count {E} exceeds int32 range; reduce max_edge_length")
-        cap = E
-    raise RuntimeError("edge enumeration did not converge")
+    return enumerate_segments(points, seg, seg_dev, int(L.query("ph_cloud_tiles", n)), cap, screen, stats)
 
 
 def sort_edges(ei: Tensor, ej: Tensor, ed: Tensor, n: int):

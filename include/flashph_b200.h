@@ -80,6 +80,29 @@ int ph_batch_edges_enumerate(const float* pts, const ph_cloud_seg* segs, int32_t
                              int32_t* out_i, int32_t* out_j, float* out_dsq, int64_t capacity,
                              unsigned long long* d_count, void* stream);
 
+/* ph_batch_edges_enumerate with a tensor-core screen (d <= 252): every
+ * cloud is centred on its mean and rounded to BF16, 128 x 128 point tiles
+ * of an augmented Gram matrix (|y_i|^2 + |y_j|^2 - 2 y_i.y_j) are formed by
+ * tcgen05.mma into tensor memory, and each value is compared with the
+ * threshold widened by a certified bound on the BF16 rounding of the points
+ * and the FP32 accumulation; the surviving pairs are recomputed with the
+ * exact FP32 chain of ph_edges_enumerate. The edge set and dist^2 bits are
+ * those of the direct kernel (the emission order differs, as it does between
+ * runs of either kernel). blk_off (nsegs+1, device): per-cloud offsets of
+ * 128-point blocks, nblocks their total; N the number of points; max_d the
+ * largest d. d_status gets PH_ERR_ITER_LIMIT if a bounded wait for the
+ * tensor cores gives up. d_stats (2 x u64, device, may be null) accumulates
+ * the pairs that passed the screen and the pairs of tiles recomputed without
+ * it (non-finite or huge coordinates, huge thresholds).
+ * Replaces the same call site as ph_batch_edges_enumerate. */
+size_t ph_edges_screened_workspace_bytes(int64_t N, int32_t nsegs, int32_t max_d);
+int ph_batch_edges_enumerate_screened(const float* pts, const ph_cloud_seg* segs, int32_t nsegs,
+                                      int64_t ntiles, int32_t max_d, int64_t N, const int64_t* blk_off,
+                                      int64_t nblocks, int32_t* out_i, int32_t* out_j, float* out_dsq,
+                                      int64_t capacity, unsigned long long* d_count, int* d_status,
+                                      unsigned long long* d_stats, void* workspace, size_t workspace_bytes,
+                                      void* stream);
+
 /* Orders E edges by the reference's packed key
  *   (float bits of dist^2) << 32 | (j(j-1)/2 + i) & 0xFFFFFFFF
  * stably with respect to the reference kernel's emission order (tiles of 32
