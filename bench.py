@@ -5,7 +5,7 @@ max_edge_length=1.4, max_dim=2 (the reference's "20K x 10 H0-H2 ms"
 figure). Synthetic data. One step = one full rips_persistence call.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {flashph,reference}]
-                  [--workload {plain,batch,serve}]
+                  [--workload {plain,batch,serve,precision}]
 
 The default line also carries a ``serving`` block: a seeded sample of the
 serving request stream (n log-uniform in [100, 50000], d in {4, 10, 50},
@@ -15,6 +15,10 @@ rips_persistence: throughput with every request queued at once, and p50/p99
 latency under Poisson arrivals at half the plain path's capacity.
 ``--workload batch`` runs the batching configuration (4096 clouds);
 ``--workload serve`` runs the serving stream over a rate sweep.
+``--workload precision`` runs the precision configuration (200000 x 50,
+max_edge_length 6.0, max_dim 1; ``--n/--d/--t/--max-dim`` override): the
+tensor-core screened edge kernel against the direct FP32 kernel, and the
+FP64 error of the diagrams.
 
 Prints one JSON line on rank 0. ``value`` is the device-timed ms per call
 with the points resident in HBM; ``e2e`` is the same call made through the
@@ -291,6 +295,144 @@ def run_serving(args, rank, local):
                                                  "t = 95th pct 20-NN, H2 for 20%"}, "serving": out}), flush=True)
 
 
+def _fp64_errors(pts64, filt, dgms):
+    """Max |value - FP64 length of its critical edge| per diagram.
+
+    Every finite birth/death value is sqrt_rn(dist^2) of an edge; the FP64
+    length of that edge is recomputed from the points. Values shared by
+    several edges take the largest error among them (an upper bound)."""
+    import torch
+    from flashph_b200.rips import edge_filtration_values
+
+    ev = edge_filtration_values(filt.edge_dist_sq)  # ascending (filtration order)
+    i, j = filt.edge_i.long(), filt.edge_j.long()
+    l64 = torch.empty(ev.shape[0], dtype=torch.float64, device=ev.device)
+    for s in range(0, ev.shape[0], 1 << 20):
+        e = slice(s, s + (1 << 20))
+        l64[e] = (pts64[i[e]] - pts64[j[e]]).pow(2).sum(1).sqrt()
+    err = (ev.double() - l64).abs()
+    rel = err / l64.clamp_min(1e-300)
+    out = {"edges": {"max_abs": float(err.max()) if err.numel() else 0.0,
+                     "max_rel": float(rel.max()) if rel.numel() else 0.0}}
+    # largest error within each run of equal fp32 values
+    uniq, inv = torch.unique_consecutive(ev, return_inverse=True)
+    grp = torch.zeros(uniq.shape[0], dtype=torch.float64, device=ev.device).scatter_reduce(
+        0, inv, err, reduce="amax")
+    for dim, dg in enumerate(dgms):
+        v = dg.reshape(-1)
+        v = v[torch.isfinite(v) & (v > 0)]
+        if v.numel() == 0:
+            out[f"H{dim}"] = {"values": 0, "max_abs": 0.0}
+            continue
+        k = torch.searchsorted(uniq, v).clamp_max(uniq.shape[0] - 1)
+        assert bool((uniq[k] == v).all()), "a diagram value is not an edge length"
+        out[f"H{dim}"] = {"values": int(v.numel()), "max_abs": float(grp[k].max())}
+    return out
+
+
+def run_precision(args, rank, local):
+    """Precision form: rips_persistence on n x d N(0,1) points (default
+    200000 x 50, max_edge_length 6.0, max_dim 1). Edge enumeration with the
+    tensor-core screen against the direct FP32 kernel on the same GPU (edge
+    sets must be identical), the full call device-timed and end to end, and
+    the FP64 error of the diagrams' critical edge lengths."""
+    import torch
+    from flashph_b200 import _edges, _lib, _timing, rips_persistence
+    from flashph_b200.rips import enumerate_edges, rips_filtration
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, d, t, md = args.n or 200000, args.d or 50, args.t or 6.0, 1 if args.max_dim is None else args.max_dim
+    pts_np = np.random.default_rng(SEED + rank).standard_normal((n, d)).astype(np.float32)
+    pts = torch.from_numpy(pts_np).to(dev)
+    pinned = torch.from_numpy(pts_np).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            r = fn()
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.mean(ts), r
+
+    def canon(e):
+        i, j, dsq = e
+        key = i.long() * n + j.long()
+        o = torch.argsort(key)
+        return key[o], dsq[o].view(torch.int32)
+
+    scr_ms, es = timed(lambda: enumerate_edges(pts, t, screen=True, stats=True), max(3, args.steps))
+    stats = dict(_edges.last_screen_stats)
+    dir_ms, ed = timed(lambda: enumerate_edges(pts, t, screen=False), 3)
+    ka, da = canon(es)
+    kb, db = canon(ed)
+    identical = bool(ka.shape == kb.shape and torch.equal(ka, kb) and torch.equal(da, db))
+
+    steps = max(3, args.steps)
+    for _ in range(max(args.warmup, 3)):
+        rips_persistence(pts, t, max_dim=md)
+    torch.cuda.synchronize()
+    l0 = _lib.launch_count()
+    with ClockSampler(local) as clocks, _timing.record() as stages:
+        ms, out = timed(lambda: rips_persistence(pts, t, max_dim=md), steps)
+    launches = (_lib.launch_count() - l0) // (steps + 1)
+    e2e_ms, res = timed(lambda: rips_persistence(pinned, t, max_dim=md), max(3, steps // 2))
+    st = _timing.summarize(stages)
+
+    pairs = n * (n - 1) // 2
+    nt = (n + 127) // 128
+    tiles = nt * (nt + 1) // 2
+    kq = ((d + 4 + 15) // 16) * 16
+    tc_flops = 2.0 * 128 * 128 * kq * tiles
+    pk, src = peaks()
+    bf16_peak = pk.get("bf16_tflops", 1590.0)
+    filt = rips_filtration(pts, t)
+    errs = _fp64_errors(pts.double(), filt, out)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        oracle.build()
+        m = min(n, 40000)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.run(pts_np[:m], t, md, fused=True, nthreads=cores)
+        sec = time.perf_counter() - t0
+        scale = (n * (n - 1)) / (m * (m - 1))
+        cpu = {"value": round(sec * 1e3 * scale, 1), "unit": "ms", "cores": cores, "kind": "port",
+               "sample": f"C++ port of the reference algorithm on the first {m} points "
+                         f"({sec:.2f} s), scaled by the pair count to n={n}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"{n // 1000}Kx{d} H0-H{md} ms (precision form)", "value": round(ms, 3), "unit": "ms",
+            "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 3), "higher_is_better": False,
+            "dtype": "f32 (bf16 screen)", "data": "synthetic",
+            "config": {"workload": f"rips_persistence, n={n} d={d} N(0,1) seed {SEED}, max_edge_length={t}, "
+                                   f"max_dim={md}", "l2": "flushed before every timed call (256 MiB write)"},
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(pinned.numel() * 4),
+                    "d2h_bytes_per_step": int(sum(r.numel() * 4 for r in res))},
+            "gpu_launches": int(launches),
+            "edges": {"E": int(ka.shape[0]), "pairs": pairs, "screened_ms": round(scr_ms, 3),
+                      "direct_ms": round(dir_ms, 3), "speedup": round(dir_ms / scr_ms, 2),
+                      "identical_to_direct": identical, "screen_candidates": stats["candidates"],
+                      "forced_pairs": stats["forced"],
+                      "candidates_per_edge": round(stats["candidates"] / max(1, int(ka.shape[0])), 3)},
+            "tensor": {"mma_flops": tc_flops, "tflops": round(tc_flops / (scr_ms * 1e-3) / 1e12, 2),
+                       "peak_bf16_tflops": bf16_peak, "frac": round(tc_flops / (scr_ms * 1e-3) / 1e12 / bf16_peak, 4),
+                       "peak_source": src},
+            "stages_ms": {k: round(v[1] / max(v[0], 1), 4) for k, v in st.items()},
+            "fp64_error": errs,
+            "rows": [int(o.shape[0]) for o in out],
+            "cpu_baseline": cpu, "clocks": clocks.summary()}), flush=True)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -339,8 +481,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=96)
-    ap.add_argument("--workload", choices=("plain", "batch", "serve"), default="plain")
+    ap.add_argument("--workload", choices=("plain", "batch", "serve", "precision"), default="plain")
     ap.add_argument("--clouds", type=int, default=4096)
+    ap.add_argument("--n", type=int, default=None, help="precision workload: points")
+    ap.add_argument("--d", type=int, default=None, help="precision workload: dimension")
+    ap.add_argument("--t", type=float, default=None, help="precision workload: max_edge_length")
+    ap.add_argument("--max-dim", type=int, default=None, help="precision workload: max_dim")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -351,6 +497,9 @@ def main():
         return
     if args.workload == "serve":
         run_serving(args, rank, local)
+        return
+    if args.workload == "precision":
+        run_precision(args, rank, local)
         return
 
     import torch
@@ -457,6 +606,7 @@ def main():
                          "peak_source": f"148 SMs x 128 FP32 lanes x 2 x sm_max_mhz ({src} peaks file)"},
             "cpu_baseline": cpu,
             "clocks": cs,
+            "stages_ms": {k: round(v[1] / max(v[0], 1), 4) for k, v in st.items()},
         }
         if not args.no_serving:
             line["serving"] = serving_summary(args.serving_requests, rates_rel=(0.5,))

@@ -29,9 +29,14 @@
 namespace ph {
 namespace {
 
-constexpr int RD_NT = 256;
+// Few warps with large shared buffers: the reduction is bound by the latency
+// of its dependency chains, not by parallel width, and a working column that
+// outgrows its shared buffer falls back to global memory (slow binary
+// searches), so the buffers are sized to hold long columns.
+constexpr int RD_NT = 128;
 constexpr int RD_WARPS = RD_NT / 32;
-constexpr int RD_CAP = 512;  // per-warp shared buffer (entries)
+constexpr int RD_CAP = 4096;  // per-warp shared buffers (entries): two working copies + the added column
+constexpr size_t RD_SMEM = (size_t)RD_WARPS * 3 * RD_CAP * sizeof(int32_t);
 constexpr unsigned FULL = 0xffffffffu;
 constexpr u64 D_CSR = 1ull << 63;
 constexpr u64 D_OFF = (1ull << 40) - 1;
@@ -168,9 +173,10 @@ __device__ __forceinline__ unsigned long long pool_alloc(RedCtl* ctl, i64 cap, i
 __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i32 row_base,
                                                  const i32* __restrict__ resid, u64* desc, i32* owner, i32* pool,
                                                  i64 pool_cap, RedCtl* ctl, int* status, int max_steps) {
-  __shared__ i32 sW[RD_WARPS][2][RD_CAP];
-  __shared__ i32 sB[RD_WARPS][RD_CAP];
+  extern __shared__ i32 rd_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  i32* sWw[2] = {rd_smem + (size_t)w * 3 * RD_CAP, rd_smem + (size_t)w * 3 * RD_CAP + RD_CAP};
+  i32* sBw = rd_smem + (size_t)w * 3 * RD_CAP + 2 * RD_CAP;
   const int nres = ctl->nres;
   volatile u64* vdesc = desc;
   volatile i32* vowner = owner;
@@ -182,7 +188,7 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i
     if (idx >= nres || *vabort) break;
     i32 c = resid[idx];
     u64 dc = vdesc[c];
-    // working column: shared buffer sW[w][cur] or, when too long, global
+    // working column: shared buffer sWw[cur] or, when too long, global
     int cur = 0;
     int k = dlen(dc);
     const i32* W;
@@ -192,9 +198,9 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i
       k = dlen(d);
       const i32* src = dptr(d, cof, pool);
       if (k <= RD_CAP) {
-        for (int i = lane; i < k; i += 32) sW[w][cur][i] = __ldcg(src + i);
+        for (int i = lane; i < k; i += 32) sWw[cur][i] = __ldcg(src + i);
         __syncwarp();
-        W = sW[w][cur];
+        W = sWw[cur];
         wg = false;
       } else {
         W = src;
@@ -257,9 +263,9 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i
       const i32* B;
       bool bg;
       if (lb <= RD_CAP) {
-        for (int i = lane; i < lb; i += 32) sB[w][i] = __ldcg(Bsrc + i);
+        for (int i = lane; i < lb; i += 32) sBw[i] = __ldcg(Bsrc + i);
         __syncwarp();
-        B = sB[w];
+        B = sBw;
         bg = false;
       } else {
         B = Bsrc;
@@ -269,7 +275,7 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i
       bool og;
       unsigned long long at = 0;
       if (k + lb <= RD_CAP) {
-        out = sW[w][cur ^ 1];
+        out = sWw[cur ^ 1];
         og = false;
       } else {
         at = pool_alloc(ctl, pool_cap, k + lb, status);
@@ -289,7 +295,7 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i
         published = true;
       } else {
         cur ^= 1;
-        W = sW[w][cur];
+        W = sWw[cur];
         wg = false;
         published = false;
       }
@@ -368,10 +374,17 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // residual count is known only on the device; K bounds it
-  const int blocks = (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * 4));
+  if (cudaFuncSetAttribute(k_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RD_SMEM) != cudaSuccess) {
+    PH_CHECK_LAUNCH();
+    return PH_ERR_CUDA;
+  }
+  int occ = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_reduce, RD_NT, RD_SMEM);
+  // residual count is known only on the device; K bounds it. Blocks are
+  // persistent (a shared work counter), so only resident blocks are launched.
+  const int blocks = (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
   ph::count_launch();
-  k_reduce<<<blocks, RD_NT, 0, s>>>(cof_data, row_base, resid, desc, owner, pool, pool_cap, ctl, d_status,
+  k_reduce<<<blocks, RD_NT, RD_SMEM, s>>>(cof_data, row_base, resid, desc, owner, pool, pool_cap, ctl, d_status,
                                     1 << 24);
   ph::count_launch();
   k_finish<<<grid_for(K), 256, 0, s>>>(cof_data, pool, resid, desc, col_state, col_piv, ctl, d_info);

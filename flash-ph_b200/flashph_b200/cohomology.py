@@ -19,6 +19,7 @@ import torch
 from torch import Tensor
 
 from . import _lib as L
+from . import _timing
 
 PH_ERR_POOL = 5
 _MAX_POOL_RETRIES = 4
@@ -158,14 +159,17 @@ def _reduce_to_rows(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, filt
 def h1_diagram(filt, edge_filt: Tensor, mst_mask: Tensor, max_triangles: int = 10_000_000, checks=()):
     """H1 rows in the reference's order, plus what H2 needs."""
     E = filt.edge_i.shape[0]
-    tris = enumerate_triangles(filt, max_triangles)
+    with _timing.stage("h1.triangles"):
+        tris = enumerate_triangles(filt, max_triangles)
     T = tris.T
-    off, data = cofacet_csr(E, E, T, 3, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb) if T else (
-        torch.zeros(E + 1, dtype=torch.int32, device=edge_filt.device),
-        torch.empty(0, dtype=torch.int32, device=edge_filt.device))
-    cmf = cof_max_face(T, 3, 0, mst_mask, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb)
-    rows, red, info = _reduce_to_rows(off, data, E, 0, T, E, mst_mask, cmf, edge_filt, None, tris.tri_m,
-                                      checks=checks)
+    with _timing.stage("h1.cofacets"):
+        off, data = cofacet_csr(E, E, T, 3, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb) if T else (
+            torch.zeros(E + 1, dtype=torch.int32, device=edge_filt.device),
+            torch.empty(0, dtype=torch.int32, device=edge_filt.device))
+        cmf = cof_max_face(T, 3, 0, mst_mask, f0=tris.tri_m, f1=tris.tri_fa, f2=tris.tri_fb)
+    with _timing.stage("h1.reduce"):
+        rows, red, info = _reduce_to_rows(off, data, E, 0, T, E, mst_mask, cmf, edge_filt, None, tris.tri_m,
+                                          checks=checks)
     return rows, tris, red, info
 
 

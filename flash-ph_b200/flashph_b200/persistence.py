@@ -13,6 +13,7 @@ import numpy as np
 import torch
 from torch import Tensor
 
+from . import _timing
 from ._lib import check_status
 from .boruvka import boruvka_mask, h0_rows
 from .cohomology import h1_diagram, h2_diagram
@@ -90,15 +91,19 @@ def rips_persistence(
 
 def _compute(points: Tensor, t: float, max_dim: int) -> list[Tensor]:
     n = points.shape[0]
-    filt = rips_filtration(points, t)
-    edge_filt = edge_filtration_values(filt.edge_dist_sq)
-    mst_mask, _, (_, mst_status) = boruvka_mask(filt.edge_i, filt.edge_j, n)
-    h0 = h0_rows(edge_filt, mst_mask, n)
+    with _timing.stage("filtration"):
+        filt = rips_filtration(points, t)
+    with _timing.stage("h0"):
+        edge_filt = edge_filtration_values(filt.edge_dist_sq)
+        mst_mask, _, (_, mst_status) = boruvka_mask(filt.edge_i, filt.edge_j, n)
+        h0 = h0_rows(edge_filt, mst_mask, n)
     if max_dim == 0:
         check_status("ph_boruvka_mst", mst_status)
         return [h0]
-    h1, tris, red1, _ = h1_diagram(filt, edge_filt, mst_mask, checks=[("ph_boruvka_mst", mst_status)])
+    with _timing.stage("h1"):
+        h1, tris, red1, _ = h1_diagram(filt, edge_filt, mst_mask, checks=[("ph_boruvka_mst", mst_status)])
     if max_dim == 1:
         return [h0, h1]
-    h2, _, _, _ = h2_diagram(filt, edge_filt, tris, red1)
+    with _timing.stage("h2"):
+        h2, _, _, _ = h2_diagram(filt, edge_filt, tris, red1)
     return [h0, h1, h2]

@@ -103,8 +103,10 @@ def rips_filtration(points: Tensor, max_edge_length: float) -> RipsFiltration:
         return RipsFiltration(e32, e32, f32, torch.zeros(n + 1, dtype=torch.int32, device=dev),
                               e32, e32, f32, n)
     ei, ej, ed = enumerate_edges(pts, max_edge_length)
-    ei, ej, ed = sort_edges(ei, ej, ed, n)
-    ptr, idx, rank = vertex_csr(ei, ej, n)
+    with _timing.stage("sort"):
+        ei, ej, ed = sort_edges(ei, ej, ed, n)
+    with _timing.stage("vertex_csr"):
+        ptr, idx, rank = vertex_csr(ei, ej, n)
     return RipsFiltration(ei, ej, ed, ptr, idx, rank, f32, n)
 
 

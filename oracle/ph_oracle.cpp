@@ -37,6 +37,7 @@ struct Result {
   // H1 (reduce_h1_gpu.py:438-604)
   i64 T = 0, cofacet_nnz = 0, n_apparent = 0, residual = 0;
   i64 xor_ops = 0, xor_max = 0, xor_elems = 0;  // reduction work statistics
+  i64 crit_path = 0;  // H1: longest chain of dependent additions (each waits for the column it adds)
   std::vector<i32> tri_max_rank_sorted;
   std::vector<i32> ap_births, ap_deaths, res_births, res_deaths, ess_births;
   std::vector<i32> h1_all_pivots;
@@ -397,6 +398,7 @@ void h1_native(Result& R, i64 n, const CSR& g, const Triangles& tr, const std::v
   }
   std::vector<char> is_app(E, 0);
   std::map<i32, Col> table;
+  std::map<i32, i64> done_at;  // pivot -> step at which its column became final
   for (i64 e = 0; e < E; ++e) {
     if (cof[e].empty() || mst_mask[e]) continue;
     if (cmf[cof[e][0]] == (i32)e) {
@@ -420,20 +422,24 @@ void h1_native(Result& R, i64 n, const CSR& g, const Triangles& tr, const std::v
       continue;
     }
     cur = cof[e];
-    i64 ops = 0;
+    i64 ops = 0, step = 0;
     while (!cur.empty()) {
       auto it = table.find(cur[0]);
       if (it == table.end()) break;
+      auto dt = done_at.find(cur[0]);
+      step = std::max(step, dt == done_at.end() ? (i64)0 : dt->second) + 1;
       R.xor_elems += (i64)(cur.size() + it->second.size());
       xor_into(cur, it->second, tmp);
       ++ops;
     }
+    R.crit_path = std::max(R.crit_path, step);
     R.xor_ops += ops;
     R.xor_max = std::max(R.xor_max, ops);
     if (!cur.empty()) {
       i32 piv = cur[0];
       R.h1_all_pivots.push_back(piv);
       table[piv] = cur;
+      done_at[piv] = step;
       if (r2f[piv] > r2f[e]) {
         R.res_births.push_back((i32)e);
         R.res_deaths.push_back(piv);
@@ -691,6 +697,7 @@ int64_t oracle_scalar(void* h, const char* name) {
   if (s == "xor_ops") return R->xor_ops;
   if (s == "xor_max") return R->xor_max;
   if (s == "xor_elems") return R->xor_elems;
+  if (s == "crit_path") return R->crit_path;
   return -1;
 }
 
