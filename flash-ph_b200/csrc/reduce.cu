@@ -15,12 +15,22 @@
 // each warp takes a residual column, keeps it in shared memory and adds the
 // column that owns its current pivot while that owner is a larger column.
 // When the pivot is free or held by a smaller column, the warp publishes the
-// column (immutable pool copy, then its descriptor, then a fence) and claims
-// the pivot with atomicMax. A smaller column it displaces is taken over by the
-// same warp and reduced further. No warp ever waits for another; every loop
-// is bounded; running out of pool sets a status code. Apparent columns own
-// their pivot from the start and are never displaced (no column processed
-// before an apparent column can contain its pivot).
+// column as an immutable record and claims the pivot with one atomicMax on the
+// pivot's owner word. A smaller column it displaces is taken over by the same
+// warp and reduced further. No warp ever waits for another; every loop is
+// bounded; running out of pool sets a status code. Apparent columns own their
+// pivot from the start and are never displaced (no column processed before an
+// apparent column can contain its pivot).
+//
+// Memory layout. Every column content lives in an immutable record
+// [len, rank_0 < rank_1 < ...] in one pool (initial records are copies of the
+// cofacet lists; later ones are bump-allocated per warp). The owner word of a
+// pivot row is (column + 1) << 33 | record offset, 0 when free, so one
+// atomicMax both orders claims by column and publishes the claimer's content:
+// a reader needs the owner word and the record, two dependent loads. Claims
+// are acquire-release atomics and owner loads are acquire loads, so no full
+// fences are needed. The final pivot of each residual column is read from the
+// owner table after the kernel.
 #include <algorithm>
 #include <climits>
 
@@ -31,16 +41,17 @@ namespace {
 
 // Few warps with large shared buffers: the reduction is bound by the latency
 // of its dependency chains, not by parallel width, and a working column that
-// outgrows its shared buffer falls back to global memory (slow binary
-// searches), so the buffers are sized to hold long columns.
+// outgrows its shared buffer falls back to global memory.
 constexpr int RD_NT = 128;
 constexpr int RD_WARPS = RD_NT / 32;
-constexpr int RD_CAP = 4096;  // per-warp shared buffers (entries): two working copies + the added column
-constexpr size_t RD_SMEM = (size_t)RD_WARPS * 3 * RD_CAP * sizeof(int32_t);
+constexpr int RD_CAP = 6144;   // per-warp shared working-column copies (entries, two of them)
+constexpr int RD_CAPB = 2048;  // per-warp shared buffer of the added column
+constexpr int RD_WSTRIDE = 2 * RD_CAP + RD_CAPB;
+constexpr size_t RD_SMEM = (size_t)RD_WARPS * RD_WSTRIDE * sizeof(int32_t);
 constexpr unsigned FULL = 0xffffffffu;
-constexpr u64 D_CSR = 1ull << 63;
-constexpr u64 D_OFF = (1ull << 40) - 1;
-constexpr int D_LEN_MAX = (1 << 23) - 1;
+constexpr int RD_FETCH = 8;  // columns a warp takes from the descending sweep at a time
+constexpr int OW_SHIFT = 33;
+constexpr u64 OW_OFF = (1ull << OW_SHIFT) - 1;
 
 struct RedCtl {
   int nres;
@@ -52,40 +63,82 @@ struct RedCtl {
   unsigned long long takeovers;
 };
 
-// Column descriptor: bit 63 = content in the cofacet CSR (else in the pool),
-// bits 40..62 = length, bits 0..39 = offset.
-__device__ __forceinline__ u64 pack_desc(bool csr, u64 len, u64 off) {
-  return (csr ? D_CSR : 0ull) | (len << 40) | off;
-}
-__device__ __forceinline__ int dlen(u64 d) { return (int)((d >> 40) & (u64)D_LEN_MAX); }
-__device__ __forceinline__ const i32* dptr(u64 d, const i32* cof, const i32* pool) {
-  return ((d & D_CSR) ? cof : pool) + (d & D_OFF);
+__device__ __forceinline__ u64 owner_word(i32 c, u64 off) { return ((u64)(c + 1) << OW_SHIFT) | off; }
+__device__ __forceinline__ i32 owner_col(u64 w) { return (i32)(w >> OW_SHIFT) - 1; }
+
+__device__ __forceinline__ u64 ld_acquire(const u64* p) {
+  u64 v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
 }
 
+__device__ __forceinline__ u64 atom_max_acq_rel(u64* p, u64 v) {
+  u64 old;
+  asm volatile("atom.acq_rel.gpu.global.max.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
+
+// Classifies columns; gives every non-empty column an initial record; apparent
+// columns own their pivot; residual columns (state 2) are left for the
+// reducer. Record space is taken with one atomic per warp.
 __global__ void k_classify(const i32* __restrict__ off, const i32* __restrict__ cof, i64 K, i32 col_base,
                            i32 row_base, const uint8_t* __restrict__ skip, const i32* __restrict__ cmf,
-                           i32* __restrict__ state, i32* __restrict__ piv, i32* __restrict__ owner,
-                           i32* __restrict__ resid, u64* __restrict__ desc, RedCtl* ctl, int* status) {
-  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x) {
-    const i32 o0 = off[c], o1 = off[c + 1];
-    if (o1 - o0 > D_LEN_MAX) set_status(status, PH_ERR_OVERFLOW);
-    desc[c] = pack_desc(true, (u64)(o1 - o0), (u64)o0);
-    if (skip && skip[c]) {
-      state[c] = 0;
-      piv[c] = -1;
-    } else if (o0 == o1) {
+                           i32* __restrict__ state, i32* __restrict__ piv, u64* __restrict__ owner,
+                           u64* __restrict__ rec, i32* __restrict__ pool, i64 pool_cap, RedCtl* ctl, int* status) {
+  const int lane = threadIdx.x & 31;
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 c0 = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); c0 < K; c0 += stride) {
+    const i64 c = c0 + lane;
+    int len = 0;
+    bool skipped = false, resid_col = false;
+    i32 o0 = 0, t = 0;
+    if (c < K) {
+      o0 = off[c];
+      len = off[c + 1] - o0;
+      skipped = skip && skip[c];
+      if (skipped) {
+        state[c] = 0;
+        piv[c] = -1;
+      } else if (len == 0) {
+        state[c] = 3;
+        piv[c] = -1;
+      } else {
+        t = cof[o0];
+        resid_col = cmf[t - row_base] != col_base + (i32)c;
+      }
+    }
+    const bool has = c < K && !skipped && len > 0;
+    // warp prefix of record sizes
+    int need = has ? len + 1 : 0, incl = need;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    unsigned long long base = 0;
+    if (lane == 31 && total) base = atomicAdd(&ctl->pool_top, (unsigned long long)total);
+    base = __shfl_sync(FULL, base, 31);
+    const u32 rm = __ballot_sync(FULL, resid_col);
+    if (lane == 0 && rm) atomicAdd(&ctl->nres, __popc(rm));
+    if (!has) continue;
+    const unsigned long long at = base + (unsigned long long)(incl - need);
+    if (base + (unsigned long long)total > (unsigned long long)pool_cap) {
+      set_status(status, PH_ERR_POOL);
+      atomicExch(&ctl->abort, 1);
       state[c] = 3;
       piv[c] = -1;
-    } else {
-      const i32 t = cof[o0];
+      continue;
+    }
+    pool[at] = len;
+    for (int i = 0; i < len; ++i) pool[at + 1 + i] = cof[o0 + i];
+    if (!resid_col) {
+      state[c] = 1;
       piv[c] = t;
-      if (cmf[t - row_base] == col_base + (i32)c) {
-        state[c] = 1;
-        owner[t - row_base] = (i32)c;
-      } else {
-        state[c] = 2;
-        resid[atomicAdd(&ctl->nres, 1)] = (i32)c;
-      }
+      owner[t - row_base] = owner_word((i32)c, at);
+    } else {
+      state[c] = 2;
+      rec[c] = at;
     }
   }
 }
@@ -97,173 +150,357 @@ __device__ __forceinline__ i32 ld(const i32* p) {
   return *p;
 }
 
-template <bool G>
-__device__ __forceinline__ int lower_bound_t(const i32* a, int n, i32 x) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (ld<G>(a + mid) < x) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-// out = A xor B for sorted lists of distinct ranks, computed by the whole
-// warp: every element looks itself up in the other list; a surviving a_i
-// goes to position i + lower_bound_B(a_i) - 2 * #(a_k in B, k < i), and
-// symmetrically for B. Returns the (warp-uniform) output length.
-template <bool AG, bool BG>
-__device__ int warp_symdiff(const i32* A, int na, const i32* B, int nb, i32* out) {
+// out = L xor S for L (<= 32 MR entries) and S (ns <= 32, one per lane in sv)
+// with everything in registers: L is loaded 32 entries per round, S_j is
+// ranked in L by ballots, and each L entry counts the insertion points below
+// it with broadcast shuffles (independent, so their latencies overlap).
+template <bool G, int MR>
+__device__ int warp_xor_tiny(const i32* L, int nl, i32 sv, int ns, i32* out) {
   const int lane = threadIdx.x & 31;
   const u32 lt = lanemask_lt();
-  int common = 0;
-  for (int base = 0; base < na; base += 32) {
-    const int i = base + lane;
-    bool in = false;
-    int lb = 0;
-    i32 x = 0;
-    if (i < na) {
-      x = ld<AG>(A + i);
-      lb = lower_bound_t<BG>(B, nb, x);
-      in = lb < nb && ld<BG>(B + lb) == x;
-    }
-    const u32 m = __ballot_sync(FULL, in);
-    const int ci = common + __popc(m & lt);
-    if (i < na && !in) out[i + lb - 2 * ci] = x;
-    common += __popc(m);
+  i32 lr[MR];
+#pragma unroll
+  for (int m = 0; m < MR; ++m) lr[m] = (lane + 32 * m < nl) ? ld<G>(L + lane + 32 * m) : INT_MAX;
+  int c[MR], dc[MR];
+  bool del[MR];
+#pragma unroll
+  for (int m = 0; m < MR; ++m) {
+    c[m] = 0;
+    dc[m] = 0;
+    del[m] = false;
   }
-  int cb = 0;
-  for (int base = 0; base < nb; base += 32) {
-    const int j = base + lane;
-    bool in = false;
-    int la = 0;
-    i32 y = 0;
-    if (j < nb) {
-      y = ld<BG>(B + j);
-      la = lower_bound_t<AG>(A, na, y);
-      in = la < na && ld<AG>(A + la) == y;
+  int mypos = nl;
+  bool mydup = false;
+  for (int j = 0; j < ns; ++j) {
+    const i32 s = __shfl_sync(FULL, sv, j);
+    int pj = 0;
+    bool eq = false;
+#pragma unroll
+    for (int m = 0; m < MR; ++m) {
+      if (32 * m < nl) {
+        pj += __popc(__ballot_sync(FULL, lr[m] < s));
+        eq |= __ballot_sync(FULL, lr[m] == s) != 0;
+      }
     }
-    const u32 m = __ballot_sync(FULL, in);
-    const int dj = cb + __popc(m & lt);
-    if (j < nb && !in) out[j + la - 2 * dj] = y;
-    cb += __popc(m);
+    if (lane == j) {
+      mypos = pj;
+      mydup = eq;
+    }
+#pragma unroll
+    for (int m = 0; m < MR; ++m) {
+      const int i = lane + 32 * m;
+      const bool le = pj <= i;
+      c[m] += le;
+      dc[m] += (eq && le);
+      del[m] |= (eq && pj == i);
+    }
   }
-  return na + nb - 2 * common;
+  const u32 dm = __ballot_sync(FULL, lane < ns && mydup);
+  if (lane < ns && !mydup) out[mypos + lane - 2 * __popc(dm & lt)] = sv;
+#pragma unroll
+  for (int m = 0; m < MR; ++m) {
+    const int i = lane + 32 * m;
+    if (i < nl && !del[m]) out[i + c[m] - 2 * dc[m]] = lr[m];
+  }
+  return nl + ns - 2 * __popc(dm);
+}
+
+// out = L xor S for a sorted list L of distinct ranks and a sorted list S of
+// at most 32 distinct ranks held one per lane (sv; INT_MAX beyond ns) -- the
+// common shape: a long working column and a short added one. Lane j finds S_j
+// in L by binary search; S_j lands at pos_j + j - 2 D_j (D_j = duplicates
+// among S_0..S_{j-1}), and L splits into ns + 1 segments between the insertion
+// points, each moved by one constant shift: the warp copies long segments one
+// after another, short ones 32 elements at a time. Returns the (warp-uniform)
+// output length.
+template <bool G>
+__device__ int warp_xor_small(const i32* L, int nl, i32 sv, int ns, i32* out) {
+  if (ns * ((nl + 31) >> 5) <= 64) {
+    if (nl <= 32) return warp_xor_tiny<G, 1>(L, nl, sv, ns, out);
+    if (nl <= 64) return warp_xor_tiny<G, 2>(L, nl, sv, ns, out);
+    if (nl <= 128) return warp_xor_tiny<G, 4>(L, nl, sv, ns, out);
+    if (nl <= 256) return warp_xor_tiny<G, 8>(L, nl, sv, ns, out);
+  }
+  const int lane = threadIdx.x & 31;
+  const u32 lt = lanemask_lt();
+  const bool act = lane < ns;
+  int pos = nl;
+  if (act) {
+    int lo = 0, hi = nl;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ld<G>(L + mid) < sv) lo = mid + 1;
+      else hi = mid;
+    }
+    pos = lo;
+  }
+  const bool dup = act && pos < nl && ld<G>(L + pos) == sv;
+  const u32 dm = __ballot_sync(FULL, dup);
+  if (act && !dup) out[pos + lane - 2 * __popc(dm & lt)] = sv;
+  if (nl >= 64 * (ns + 1)) {
+    // long segments: the warp copies segment k = 0..ns in turn, moved by k - 2 D_k
+    const int pprev = __shfl_up_sync(FULL, pos, 1);
+    const int start = lane == 0 ? 0 : pprev + (int)((dm >> (lane - 1)) & 1u);
+    for (int k = 0; k <= ns && k < 32; ++k) {
+      const int a = __shfl_sync(FULL, start, k);
+      const int b = k == ns ? nl : __shfl_sync(FULL, pos, k);
+      const int sh = k - 2 * __popc(dm & ((1u << k) - 1u));
+      for (int i = a + lane; i < b; i += 32) out[i + sh] = ld<G>(L + i);
+    }
+    if (ns == 32) {  // segment 32 (after the last insertion point)
+      const int a = __shfl_sync(FULL, pos, 31) + (int)(dm >> 31), sh = 32 - 2 * __popc(dm);
+      for (int i = a + lane; i < nl; i += 32) out[i + sh] = ld<G>(L + i);
+    }
+  } else {
+    // short segments: 32 elements of L at a time; c = #{j : pos_j <= i} by
+    // broadcast shuffles of the insertion points, L[i] deleted when S_{c-1} is
+    // its twin, else moved by c - 2 D_c
+    for (int i0 = 0; i0 < nl; i0 += 32) {
+      const int i = i0 + lane;
+      int c = 0;
+      for (int j = 0; j < ns; ++j) c += __shfl_sync(FULL, pos, j) <= i;
+      const int plast = __shfl_sync(FULL, pos, (c + 31) & 31);
+      const u32 below = c >= 32 ? FULL : ((1u << c) - 1u);
+      const bool deleted = c > 0 && ((dm >> (c - 1)) & 1u) && plast == i;
+      if (i < nl && !deleted) out[i + c - 2 * __popc(dm & below)] = ld<G>(L + i);
+    }
+  }
+  return nl + ns - 2 * __popc(dm);
+}
+
+// out = A xor B for sorted lists of distinct ranks, both longer than 32, by
+// merge path over 128 segments of the merged sequence (ties: A first): lane l
+// merges segments 4l .. 4l + 3 as four interleaved chains (independent loads
+// in flight), counting survivors in a first pass and writing them after a
+// scan. An element is dropped when its twin is in the other list; the twin of
+// A[i] can only be B[ib] and the twin of B[j] only A[ia - 1] at the merge
+// position, whichever segment they fall in. The loop is branch-free so that
+// lanes do not diverge.
+template <bool AG, bool BG>
+__device__ int warp_xor_merge(const i32* A, int na, const i32* B, int nb, i32* out) {
+  constexpr int CH = 4;
+  const int lane = threadIdx.x & 31;
+  const int total = na + nb;
+  const int per = (total + 32 * CH - 1) / (32 * CH);
+  int ia0[CH], ib0[CH], d1[CH];
+#pragma unroll
+  for (int c = 0; c < CH; ++c) {
+    const int d0 = min((lane * CH + c) * per, total);
+    d1[c] = min(d0 + per, total);
+    int lo = max(0, d0 - nb), hi = min(d0, na);
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ld<AG>(A + mid) <= ld<BG>(B + d0 - 1 - mid)) lo = mid + 1;
+      else hi = mid;
+    }
+    ia0[c] = lo;
+    ib0[c] = d0 - lo;
+  }
+  int cnt[CH] = {0, 0, 0, 0};
+  int total_out = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    int ia[CH], ib[CH], pos[CH], d[CH];
+    i32 a[CH], b[CH], pa[CH];
+    int lane_base = 0;
+    if (pass == 1) {
+      const int mine = cnt[0] + cnt[1] + cnt[2] + cnt[3];
+      int incl = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      lane_base = incl - mine;
+      total_out = __shfl_sync(FULL, incl, 31);
+    }
+    int run = lane_base;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      ia[c] = ia0[c];
+      ib[c] = ib0[c];
+      d[c] = ia0[c] + ib0[c];
+      a[c] = ia[c] < na ? ld<AG>(A + ia[c]) : INT_MAX;
+      b[c] = ib[c] < nb ? ld<BG>(B + ib[c]) : INT_MAX;
+      pa[c] = ia[c] > 0 ? ld<AG>(A + ia[c] - 1) : -1;
+      pos[c] = run;
+      run += cnt[c];
+      if (pass == 0) cnt[c] = 0;
+    }
+    for (int step = 0; step < per; ++step) {
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (d[c] >= d1[c]) continue;
+        const bool ta = ib[c] >= nb || (ia[c] < na && a[c] <= b[c]);
+        const i32 x = ta ? a[c] : b[c];
+        const bool keep = ta ? (b[c] != a[c]) : (pa[c] != b[c]);
+        if (pass == 1 && keep) out[pos[c]] = x;
+        pos[c] += keep;
+        if (pass == 0) cnt[c] += keep;
+        pa[c] = ta ? a[c] : pa[c];
+        ia[c] += ta;
+        ib[c] += !ta;
+        ++d[c];
+        const i32 an = ld<AG>(A + min(ia[c], na - 1)), bn = ld<BG>(B + min(ib[c], nb - 1));
+        a[c] = ia[c] < na ? an : INT_MAX;
+        b[c] = ib[c] < nb ? bn : INT_MAX;
+      }
+    }
+  }
+  return total_out;
 }
 
 __device__ __forceinline__ int symdiff(const i32* A, bool ag, int na, const i32* B, bool bg, int nb, i32* out) {
-  if (ag) return bg ? warp_symdiff<true, true>(A, na, B, nb, out) : warp_symdiff<true, false>(A, na, B, nb, out);
-  return bg ? warp_symdiff<false, true>(A, na, B, nb, out) : warp_symdiff<false, false>(A, na, B, nb, out);
+  const int lane = threadIdx.x & 31;
+  if (nb <= 32) {
+    const i32 sv = lane < nb ? (bg ? __ldcg(B + lane) : B[lane]) : INT_MAX;
+    return ag ? warp_xor_small<true>(A, na, sv, nb, out) : warp_xor_small<false>(A, na, sv, nb, out);
+  }
+  if (na <= 32) {
+    const i32 sv = lane < na ? (ag ? __ldcg(A + lane) : A[lane]) : INT_MAX;
+    return bg ? warp_xor_small<true>(B, nb, sv, na, out) : warp_xor_small<false>(B, nb, sv, na, out);
+  }
+  if (ag) return bg ? warp_xor_merge<true, true>(A, na, B, nb, out) : warp_xor_merge<true, false>(A, na, B, nb, out);
+  return bg ? warp_xor_merge<false, true>(A, na, B, nb, out) : warp_xor_merge<false, false>(A, na, B, nb, out);
 }
 
-// Bump allocation in the pool (lane 0), broadcast to the warp; ~0 on overflow.
-__device__ __forceinline__ unsigned long long pool_alloc(RedCtl* ctl, i64 cap, int n, int* status) {
+// Per-warp bump allocation from pool chunks (lane 0 holds the chunk); the
+// offset is broadcast to the warp, ~0 when the pool is exhausted.
+struct PoolChunk {
+  unsigned long long pos = 0, end = 0;
+};
+
+__device__ __forceinline__ unsigned long long pool_alloc(PoolChunk& ch, RedCtl* ctl, i64 cap, int n, int chunk,
+                                                         int* status) {
   unsigned long long at = 0;
   if ((threadIdx.x & 31) == 0) {
-    at = atomicAdd(&ctl->pool_top, (unsigned long long)n);
-    if (at + (unsigned long long)n > (unsigned long long)cap) {
-      set_status(status, PH_ERR_POOL);
-      atomicExch(&ctl->abort, 1);
-      at = ~0ull;
+    if (ch.pos + (unsigned long long)n <= ch.end) {
+      at = ch.pos;
+      ch.pos += n;
+    } else {
+      const int take = n > chunk / 2 ? n : chunk;
+      at = atomicAdd(&ctl->pool_top, (unsigned long long)take);
+      if (at + (unsigned long long)take > (unsigned long long)cap) {
+        set_status(status, PH_ERR_POOL);
+        atomicExch(&ctl->abort, 1);
+        at = ~0ull;
+      } else if (take > n) {
+        ch.pos = at + n;
+        ch.end = at + take;
+      }
     }
   }
   return __shfl_sync(FULL, at, 0);
 }
 
-__global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i32 row_base,
-                                                 const i32* __restrict__ resid, u64* desc, i32* owner, i32* pool,
-                                                 i64 pool_cap, RedCtl* ctl, int* status, int max_steps) {
+// Residual columns are taken in descending order (the serial algorithm's
+// order), RD_FETCH at a time per warp, so that a column mostly meets final
+// versions of the larger columns it adds and is rarely displaced.
+__global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32* __restrict__ state,
+                                                 const u64* __restrict__ rec, u64* owner, i32* pool, i64 pool_cap,
+                                                 int chunk, RedCtl* ctl, int* status, int max_steps) {
   extern __shared__ i32 rd_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  i32* sWw[2] = {rd_smem + (size_t)w * 3 * RD_CAP, rd_smem + (size_t)w * 3 * RD_CAP + RD_CAP};
-  i32* sBw = rd_smem + (size_t)w * 3 * RD_CAP + 2 * RD_CAP;
-  const int nres = ctl->nres;
-  volatile u64* vdesc = desc;
-  volatile i32* vowner = owner;
+  i32* const sW0 = rd_smem + (size_t)w * RD_WSTRIDE;  // working copies at sW0 and sW0 + RD_CAP
+  i32* const sBw = sW0 + 2 * RD_CAP;
   volatile int* vabort = &ctl->abort;
+  PoolChunk chunk_state;
+  unsigned long long n_merges = 0, n_takeovers = 0;
   for (;;) {
-    int idx = 0;
-    if (lane == 0) idx = atomicAdd(&ctl->next, 1);
-    idx = __shfl_sync(FULL, idx, 0);
-    if (idx >= nres || *vabort) break;
-    i32 c = resid[idx];
-    u64 dc = vdesc[c];
-    // working column: shared buffer sWw[cur] or, when too long, global
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&ctl->next, RD_FETCH);
+    base = __shfl_sync(FULL, base, 0);
+    if ((i64)base >= K || *vabort) break;
+    const i64 cand = K - 1 - base - lane;
+    u32 todo = __ballot_sync(FULL, lane < RD_FETCH && cand >= 0 && state[cand] == 2);
+    while (todo && !*vabort) {
+    const int l = __ffs(todo) - 1;
+    todo &= todo - 1;
+    i32 c = (i32)(K - 1 - base - l);
+    // working column: shared buffer (sW0 + cur * RD_CAP) or, when too long, a pool record
     int cur = 0;
-    int k = dlen(dc);
-    const i32* W;
-    bool wg;          // W is in global memory
-    bool published;   // dc describes W exactly (nothing to write before a claim)
-    auto load_work = [&](u64 d) {
-      k = dlen(d);
-      const i32* src = dptr(d, cof, pool);
+    int k = 0;
+    const i32* W = nullptr;
+    bool wg = false;      // W is in global memory
+    bool published = false;
+    u64 wrec = 0;         // record offset of W when published
+    auto load_record = [&](u64 at) {
+      const i32* src = pool + at + 1;
+      k = __ldcg(pool + at);
       if (k <= RD_CAP) {
-        for (int i = lane; i < k; i += 32) sWw[cur][i] = __ldcg(src + i);
+        for (int i = lane; i < k; i += 32) (sW0 + cur * RD_CAP)[i] = __ldcg(src + i);
         __syncwarp();
-        W = sWw[cur];
+        W = (sW0 + cur * RD_CAP);
         wg = false;
       } else {
         W = src;
         wg = true;
       }
-      dc = d;
+      wrec = at;
       published = true;
     };
-    load_work(dc);
+    load_record(rec[c]);
     for (int step = 0;; ++step) {
       if (step >= max_steps) {
         if (lane == 0) set_status(status, PH_ERR_ITER_LIMIT);
         atomicExch(&ctl->abort, 1);
         break;
       }
-      if (k == 0) {
-        if (lane == 0) vdesc[c] = pack_desc(false, 0, 0);
-        break;
-      }
+      if (k == 0) break;  // the column vanished: it owns nothing
       const i32 p = wg ? __ldcg(W) : W[0];
-      i32 o = vowner[p - row_base];
+      u64 ow = ld_acquire(owner + (p - row_base));
+      i32 o = owner_col(ow);
       if (o < c) {
-        // publish W, then claim p
+        // publish W as a record, then claim p
         if (!published) {
-          const unsigned long long at = pool_alloc(ctl, pool_cap, k, status);
+          const unsigned long long at = pool_alloc(chunk_state, ctl, pool_cap, k + 1, chunk, status);
           if (at == ~0ull) break;
-          for (int i = lane; i < k; i += 32) pool[at + i] = wg ? __ldcg(W + i) : W[i];
-          dc = pack_desc(false, (u64)k, at);
+          if (lane == 0) pool[at] = k;
+          for (int i = lane; i < k; i += 32) pool[at + 1 + i] = wg ? __ldcg(W + i) : W[i];
+          wrec = at;
           published = true;
         }
-        __threadfence();
         __syncwarp();
-        i32 old = 0;
-        if (lane == 0) {
-          vdesc[c] = dc;
-          __threadfence();
-          old = atomicMax(&owner[p - row_base], c);
-        }
+        u64 old = 0;
+        if (lane == 0) old = atom_max_acq_rel(owner + (p - row_base), owner_word(c, wrec));
         old = __shfl_sync(FULL, old, 0);
-        if (old < c) {
-          if (old < 0) break;  // claimed a free pivot: this work item is done
+        __syncwarp();
+        const i32 oc = owner_col(old);
+        if (oc < c) {
+          if (oc < 0) break;  // claimed a free pivot: this work item is done
           // displaced a smaller column: take it over
-          if (lane == 0) atomicAdd(&ctl->takeovers, 1ull);
-          c = old;
-          __threadfence();
-          load_work(vdesc[c]);
+          ++n_takeovers;
+          c = oc;
+          load_record(old & OW_OFF);
           continue;
         }
-        o = old;  // a larger column got there first
+        o = oc;  // a larger column got there first
+        ow = old;
       }
       if (o == c) {  // cannot happen: a column never owns a pivot it is still reducing
         if (lane == 0) set_status(status, PH_ERR_ARG);
         break;
       }
-      // add the larger owner o
-      __threadfence();
-      const u64 od = vdesc[o];
-      const int lb = dlen(od);
-      const i32* Bsrc = dptr(od, cof, pool);
+      // add the larger owner o: its record head (length + 31 entries) in one load
+      const u64 at_o = ow & OW_OFF;
+      const i32 head = (at_o + lane < (u64)pool_cap) ? __ldcg(pool + at_o + lane) : 0;
+      const int lb = __shfl_sync(FULL, head, 0);
+      const i32 bv = __shfl_down_sync(FULL, head, 1);  // entry `lane` of B (lanes < 31)
+      if (!wg && lb <= 31 && k + lb <= RD_CAP) {
+        const int m = warp_xor_small<false>(W, k, lane < lb ? bv : INT_MAX, lb, (sW0 + (cur ^ 1) * RD_CAP));
+        __syncwarp();
+        ++n_merges;
+        k = m;
+        cur ^= 1;
+        W = (sW0 + cur * RD_CAP);
+        published = false;
+        continue;
+      }
+      const i32* Bsrc = pool + at_o + 1;
       const i32* B;
       bool bg;
-      if (lb <= RD_CAP) {
-        for (int i = lane; i < lb; i += 32) sBw[i] = __ldcg(Bsrc + i);
+      if (lb <= RD_CAPB) {
+        if (lane < 31 && lane < lb) sBw[lane] = bv;
+        for (int i = 31 + lane; i < lb; i += 32) sBw[i] = __ldcg(Bsrc + i);
         __syncwarp();
         B = sBw;
         bg = false;
@@ -275,54 +512,65 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(const i32* __restrict__ cof, i
       bool og;
       unsigned long long at = 0;
       if (k + lb <= RD_CAP) {
-        out = sWw[cur ^ 1];
+        out = (sW0 + (cur ^ 1) * RD_CAP);
         og = false;
       } else {
-        at = pool_alloc(ctl, pool_cap, k + lb, status);
+        at = pool_alloc(chunk_state, ctl, pool_cap, k + lb + 1, chunk, status);
         if (at == ~0ull) break;
-        out = pool + at;
+        out = pool + at + 1;
         og = true;
       }
       const int m = symdiff(W, wg, k, B, bg, lb, out);
       __syncwarp();
-      if (lane == 0) atomicAdd(&ctl->merges, 1ull);
+      ++n_merges;
       k = m;
       if (og) {
-        __threadfence();
+        if (lane == 0) pool[at] = m;
+        __syncwarp();
         W = out;
         wg = true;
-        dc = pack_desc(false, (u64)k, at);
+        wrec = at;
         published = true;
       } else {
         cur ^= 1;
-        W = sWw[cur];
+        W = (sW0 + cur * RD_CAP);
         wg = false;
         published = false;
       }
     }
+    }
+  }
+  if (lane == 0) {
+    if (n_merges) atomicAdd(&ctl->merges, n_merges);
+    if (n_takeovers) atomicAdd(&ctl->takeovers, n_takeovers);
   }
 }
 
-__global__ void k_finish(const i32* __restrict__ cof, const i32* __restrict__ pool, const i32* __restrict__ resid,
-                         const u64* __restrict__ desc, i32* __restrict__ state, i32* __restrict__ piv,
-                         const RedCtl* ctl, i64* info) {
-  const i64 nres = ctl->nres;
-  for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < nres; r += (i64)gridDim.x * blockDim.x) {
-    const i32 c = resid[r];
-    const u64 d = desc[c];
-    if (dlen(d) == 0) {
-      state[c] = 3;
-      piv[c] = -1;
-    } else {
-      state[c] = 2;
-      piv[c] = dptr(d, cof, pool)[0];
-    }
+// residual columns default to empty (state 3) ...
+__global__ void k_finish_cols(i64 K, i32* __restrict__ state, i32* __restrict__ piv, const RedCtl* ctl, i64* info) {
+  for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x) {
+    if (state[c] != 2) continue;
+    state[c] = 3;
+    piv[c] = -1;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && info) {
     info[0] = ctl->nres;
     info[1] = (i64)ctl->merges;
     info[2] = (i64)ctl->pool_top;
     info[3] = (i64)ctl->takeovers;
+  }
+}
+
+// ... and a residual column that owns a row at the end is paired with it
+__global__ void k_finish_rows(const u64* __restrict__ owner, i64 R, i32 row_base, i32* __restrict__ state,
+                              i32* __restrict__ piv) {
+  for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < R; r += (i64)gridDim.x * blockDim.x) {
+    const u64 w = owner[r];
+    if (!w) continue;
+    const i32 c = owner_col(w);
+    if (state[c] == 1) continue;  // apparent
+    state[c] = 2;
+    piv[c] = (i32)r + row_base;
   }
 }
 
@@ -342,8 +590,7 @@ inline int grid_for(i64 n, int nt = 256) {
 using namespace ph;
 
 extern "C" size_t ph_reduce_workspace_bytes(int64_t K, int64_t R) {
-  return Carve::need((size_t)R * 4) + Carve::need((size_t)K * 4) + Carve::need((size_t)K * 8) +
-         Carve::need(sizeof(RedCtl));
+  return Carve::need((size_t)R * 8) + Carve::need((size_t)K * 8) + Carve::need(sizeof(RedCtl));
 }
 
 extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,
@@ -353,7 +600,7 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
                          void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (K < 0 || R < 0 || pool_cap < 0) return PH_ERR_ARG;
-  if (K >= (int64_t(1) << 31) || R >= (int64_t(1) << 31) || pool_cap >= (int64_t(1) << 40))
+  if (K >= (int64_t(1) << 31) || R >= (int64_t(1) << 31) || pool_cap >= (int64_t(1) << OW_SHIFT))
     return PH_ERR_OVERFLOW;
   if (K == 0) {
     if (d_info) cudaMemsetAsync(d_info, 0, 4 * sizeof(int64_t), s);
@@ -361,16 +608,15 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
     return PH_OK;
   }
   Carve c(workspace, workspace_bytes);
-  i32* owner = c.take<i32>(std::max<i64>(R, 1));
-  i32* resid = c.take<i32>(K);
-  u64* desc = c.take<u64>(K);
+  u64* owner = c.take<u64>(std::max<i64>(R, 1));
+  u64* rec = c.take<u64>(K);
   RedCtl* ctl = c.take<RedCtl>(1);
-  if (!owner || !resid || !desc || !ctl) return PH_ERR_ARG;
-  cudaMemsetAsync(owner, 0xff, sizeof(i32) * std::max<i64>(R, 1), s);
+  if (!owner || !rec || !ctl) return PH_ERR_ARG;
+  cudaMemsetAsync(owner, 0, sizeof(u64) * std::max<i64>(R, 1), s);
   cudaMemsetAsync(ctl, 0, sizeof(RedCtl), s);
   ph::count_launch();
   k_classify<<<grid_for(K), 256, 0, s>>>(cof_off, cof_data, K, col_base, row_base, skip, row_cmf, col_state,
-                                         col_piv, owner, resid, desc, ctl, d_status);
+                                         col_piv, owner, rec, pool, pool_cap, ctl, d_status);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -382,12 +628,19 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_reduce, RD_NT, RD_SMEM);
   // residual count is known only on the device; K bounds it. Blocks are
   // persistent (a shared work counter), so only resident blocks are launched.
-  const int blocks = (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
+  const int blocks =
+      (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
+  // pool chunk per warp: small enough that the chunks of all warps fit a quarter of the pool
+  const int chunk = (int)std::max<i64>(64, std::min<i64>(2048, pool_cap / (4 * (i64)blocks * RD_WARPS)));
   ph::count_launch();
-  k_reduce<<<blocks, RD_NT, RD_SMEM, s>>>(cof_data, row_base, resid, desc, owner, pool, pool_cap, ctl, d_status,
-                                    1 << 24);
+  k_reduce<<<blocks, RD_NT, RD_SMEM, s>>>(row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
+                                          1 << 24);
   ph::count_launch();
-  k_finish<<<grid_for(K), 256, 0, s>>>(cof_data, pool, resid, desc, col_state, col_piv, ctl, d_info);
+  k_finish_cols<<<grid_for(K), 256, 0, s>>>(K, col_state, col_piv, ctl, d_info);
+  if (R > 0) {
+    ph::count_launch();
+    k_finish_rows<<<grid_for(R), 256, 0, s>>>(owner, R, row_base, col_state, col_piv);
+  }
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

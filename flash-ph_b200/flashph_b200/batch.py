@@ -265,7 +265,7 @@ def _reduce_retry(off, data, K, col_base, R, row_base, skip, cmf, checks):
     """Reduction whose status is read with the final synchronisation; a pool
     overflow (rare) is detected here by a synchronous check and retried."""
     nnz = int(data.numel())
-    pool_cap = max(4 * nnz, 1 << 20)
+    pool_cap = max(16 * nnz + 2 * K, 1 << 22)
     for _ in range(4):
         red = _reduce(off, data, K, col_base, R, row_base, skip, cmf, pool_cap)
         st = int(red.status.item())

@@ -138,7 +138,7 @@ def _reduce_to_rows(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, filt
     stages, read back in the same copy and raised if non-zero.
     """
     nnz = int(cof_data.numel())
-    pool_cap = max(4 * nnz, 1 << 20)
+    pool_cap = max(16 * nnz + 2 * K, 1 << 22)
     for _ in range(_MAX_POOL_RETRIES):
         red = reduce(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, pool_cap)
         rows, nrows = persistence_rows(red, K, row_base, filt, col_m, row_m)
