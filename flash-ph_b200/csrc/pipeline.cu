@@ -1,0 +1,448 @@
+// Native orchestration of rips_persistence for one point cloud.
+//
+// Reference: persistence.py:77-215 (rips_persistence): filtration
+// (rips.py:170-200), H0 (boruvka.py, persistence.py:169-192), H1
+// (reduce_h1_gpu.py), H2 (cohomology_general.py). The stages are the
+// library's own entry points, called in order on one stream; intermediate
+// buffers come from the stream-ordered allocator and are released together.
+// The host waits only where a count decides the next allocation:
+//   1. the edge count (edge buffers are sized by an estimate, rerun if short)
+//   2. the triangle count (and the H0 forest's status)
+//   3. the H1 reduction's status and row count, together with the
+//      tetrahedron count when H2 is asked for
+//   4. the H2 reduction's status and row count
+// The results stay on the device in a ph_result until copied out.
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "prim.cuh"
+
+using namespace ph;
+
+struct ph_result {
+  float* rows[3] = {nullptr, nullptr, nullptr};
+  int64_t nrows[3] = {0, 0, 0};
+  int ndim = 0;
+  cudaStream_t stream = nullptr;
+  int64_t stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // E, T, Q, H1 additions, H2 additions
+};
+
+namespace {
+
+// stream-ordered allocations released together when the run ends
+struct Arena {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  bool failed = false;
+  explicit Arena(cudaStream_t st) : s(st) {}
+  Arena(const Arena&) = delete;
+  Arena& operator=(const Arena&) = delete;
+  template <typename T>
+  T* take(i64 count) {
+    void* p = nullptr;
+    const size_t bytes = (size_t)std::max<i64>(count, 1) * sizeof(T);
+    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) {
+      failed = true;
+      return nullptr;
+    }
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  void* bytes(size_t n) { return take<unsigned char>((i64)std::max<size_t>(n, 1)); }
+  ~Arena() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+  }
+};
+
+// small pinned host buffer per thread for count and status readbacks
+int64_t* pinned_slots() {
+  thread_local int64_t* buf = nullptr;
+  if (!buf) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, 64 * sizeof(int64_t)) != cudaSuccess) return nullptr;
+    buf = static_cast<int64_t*>(p);
+  }
+  return buf;
+}
+
+// keeps the device's stream-ordered pool from returning memory at every sync
+// (a setting of this process's pool, nothing that outlasts it)
+void keep_pool(int dev) {
+  static bool done[64] = {};
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[dev] = true;
+}
+
+// fp32 of a double, round to nearest even, inf beyond the fp32 range (numpy's float32())
+float to_f32(double v) {
+  if (std::isnan(v)) return NAN;
+  const double lim = 0x1p128 - 0x1p103;  // halfway between FLT_MAX and 2^128
+  if (v >= lim) return INFINITY;
+  if (v <= -lim) return -INFINITY;
+  return (float)v;
+}
+
+__global__ void k_single_seg(ph_cloud_seg* seg, int64_t* blk_off, int64_t n, int32_t d, float thr_sq,
+                             int64_t nblocks) {
+  ph_cloud_seg s;
+  s.pt_off = 0;
+  s.vbase = 0;
+  s.tile_off = 0;
+  s.n = (int32_t)n;
+  s.d = d;
+  s.thr_sq = thr_sq;
+  s.max_dim = 2;
+  *seg = s;
+  blk_off[0] = 0;
+  blk_off[1] = nblocks;
+}
+
+int fail(int code, const std::string& msg) {
+  record_message(msg.c_str());
+  return code;
+}
+
+// copies count int64 values (device) to the pinned slots and waits
+int readback(const int64_t* const* src, int count, int64_t* dst, cudaStream_t s) {
+  for (int k = 0; k < count; ++k)
+    if (cudaMemcpyAsync(dst + k, src[k], sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+      record_error(cudaGetLastError());
+      return PH_ERR_CUDA;
+    }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    record_error(e);
+    return PH_ERR_CUDA;
+  }
+  return PH_OK;
+}
+
+struct RedOut {
+  i32* state;
+  i32* piv;
+  int64_t* info;
+  int64_t* nrows;
+};
+
+// one reduction (H1 or H2) and its persistence rows, enqueued
+int reduce_rows(Arena& A, cudaStream_t s, const i32* off, const i32* data, i64 K, i32 col_base, i64 R,
+                i32 row_base, const uint8_t* skip, const i32* cmf, const float* filt, const i32* col_m,
+                const i32* row_m, i64 pool_cap, int* status, float* rows, RedOut& o) {
+  o.state = A.take<i32>(K);
+  o.piv = A.take<i32>(K);
+  o.info = A.take<int64_t>(4);
+  o.nrows = A.take<int64_t>(1);
+  i32* pool = A.take<i32>(pool_cap);
+  const size_t rb = ph_reduce_workspace_bytes(K, R), pb = ph_persistence_rows_workspace_bytes(K);
+  void* rws = A.bytes(rb);
+  void* pws = A.bytes(pb);
+  if (A.failed) return fail(PH_ERR_CUDA, "rips_persistence: device allocation failed");
+  PH_TRY(ph_reduce(off, data, K, col_base, R, row_base, skip, cmf, o.state, o.piv, pool, pool_cap, o.info, status,
+                   rws, rb, s));
+  return ph_persistence_rows(o.state, o.piv, K, row_base, filt, col_m, row_m, rows, o.nrows, pws, pb, s);
+}
+
+}  // namespace
+
+extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, double max_edge_length,
+                                   int32_t max_dim, int64_t max_triangles, int64_t max_tetrahedra,
+                                   int32_t edge_mode, ph_result** out, void* stream) {
+  if (!out) return PH_ERR_ARG;
+  *out = nullptr;
+  if (!d_points || n < 2 || d < 1 || max_dim < 0 || max_dim > 2 || edge_mode < 0 || edge_mode > 2 ||
+      (edge_mode == 1 && d > 252))
+    return fail(PH_ERR_ARG, "ph_rips_persistence: invalid argument");
+  if (n >= (int64_t(1) << 31)) return fail(PH_ERR_OVERFLOW, "ph_rips_persistence: n exceeds the int32 range");
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  keep_pool(dev);
+  int64_t* H = pinned_slots();
+  if (!H) return fail(PH_ERR_CUDA, "ph_rips_persistence: pinned host buffer unavailable");
+
+  Arena A(s);
+  ph_result* res = new ph_result();
+  res->stream = s;
+  res->ndim = max_dim + 1;
+  auto give_up = [&](int code) {
+    for (float* r : res->rows)
+      if (r) cudaFreeAsync(r, s);
+    delete res;
+    return code;
+  };
+  auto alloc_fail = [&]() { return give_up(fail(PH_ERR_CUDA, "ph_rips_persistence: device allocation failed")); };
+  const float thr_sq = to_f32(max_edge_length * max_edge_length);
+
+  // ---- 1. edges (rips.py:170-200; edge_kernel.py) ----------------------------------------
+  const bool screened = edge_mode == 1 || (edge_mode == 0 && d >= 8 && d <= 252);
+  const i64 nblocks = (n + 127) / 128;
+  const i64 ntiles = ph_cloud_tiles(n);
+  ph_cloud_seg* seg = A.take<ph_cloud_seg>(1);
+  int64_t* blk = A.take<int64_t>(2);
+  // cnt[0]: edge count; statuses as int32 words from cnt + 1: st[0] edges,
+  // st[1] forest, st[2] H1 reduction, st[3] tetrahedra, st[4] H2 reduction
+  int64_t* cnt = A.take<int64_t>(8);
+  if (A.failed) return alloc_fail();
+  cudaMemsetAsync(cnt, 0, 8 * sizeof(int64_t), s);
+  int* st = reinterpret_cast<int*>(cnt + 1);
+  count_launch();
+  k_single_seg<<<1, 1, 0, s>>>(seg, blk, n, d, thr_sq, nblocks);
+  const size_t ews = screened ? ph_edges_screened_workspace_bytes(n, 1, d) : 0;
+  void* ew = screened ? A.bytes(ews) : nullptr;
+  const i64 pairs = n * (n - 1) / 2;
+  i64 cap = std::min<i64>(pairs, std::max<i64>(1 << 22, 256 * n));
+  i32 *ei = nullptr, *ej = nullptr;
+  float* ed = nullptr;
+  i64 E = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    cap = std::max<i64>(cap, 1);
+    ei = A.take<i32>(cap);
+    ej = A.take<i32>(cap);
+    ed = A.take<float>(cap);
+    if (A.failed) return alloc_fail();
+    int rc;
+    if (screened)
+      rc = ph_batch_edges_enumerate_screened(d_points, seg, 1, ntiles, d, n, blk, nblocks, ei, ej, ed, cap,
+                                             reinterpret_cast<unsigned long long*>(cnt), st, nullptr, ew, ews, s);
+    else
+      rc = ph_batch_edges_enumerate(d_points, seg, 1, ntiles, ei, ej, ed, cap,
+                                    reinterpret_cast<unsigned long long*>(cnt), s);
+    if (rc != PH_OK) return give_up(rc);
+    const int64_t* src[2] = {cnt, cnt + 1};
+    if (readback(src, 2, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int st_e = (int)(H[1] & 0xffffffff);
+    if (st_e) return give_up(fail(st_e, "edge enumeration failed"));
+    E = H[0];
+    if (E <= cap || E >= (int64_t(1) << 31)) break;
+    cap = E;
+  }
+  if (E >= (int64_t(1) << 31)) {
+    char m[160];
+    snprintf(m, sizeof m, "Edge count %lld exceeds int32 range; reduce max_edge_length", (long long)E);
+    return give_up(fail(PH_ERR_LIMIT, m));
+  }
+  res->stats[0] = E;
+
+  // ---- 2. filtration order, adjacency, values ---------------------------------------------
+  i32* si = A.take<i32>(E);
+  i32* sj = A.take<i32>(E);
+  float* sd = A.take<float>(E);
+  i32* adj_ptr = A.take<i32>(n + 1);
+  i32* adj_idx = A.take<i32>(2 * E);
+  i32* adj_rank = A.take<i32>(2 * E);
+  float* filt = A.take<float>(E);
+  const size_t sort_b = ph_edges_sort_workspace_bytes(E), csr_b = ph_vertex_csr_workspace_bytes(E);
+  void* sort_ws = A.bytes(sort_b);
+  void* csr_ws = A.bytes(csr_b);
+  if (A.failed) return alloc_fail();
+  if (E) {
+    int rc = ph_edges_sort(ei, ej, ed, E, n, si, sj, sd, sort_ws, sort_b, s);
+    if (rc == PH_OK) rc = ph_vertex_csr(si, sj, E, n, adj_ptr, adj_idx, adj_rank, csr_ws, csr_b, s);
+    if (rc == PH_OK) rc = ph_sqrt_f32(sd, filt, E, s);
+    if (rc != PH_OK) return give_up(rc);
+  } else {
+    cudaMemsetAsync(adj_ptr, 0, sizeof(i32) * (n + 1), s);
+  }
+
+  // ---- 3. H0 (boruvka.py, persistence.py:169-192) ---------------------------------------------
+  uint8_t* mask = A.take<uint8_t>(E);
+  i32* comp = A.take<i32>(n);
+  int64_t* ncomp = A.take<int64_t>(1);
+  const size_t mst_b = ph_boruvka_workspace_bytes(n, E), h0_b = ph_h0_rows_workspace_bytes(E);
+  void* mst_ws = A.bytes(mst_b);
+  void* h0_ws = A.bytes(h0_b);
+  if (A.failed || cudaMallocAsync((void**)&res->rows[0], sizeof(float) * 2 * n, s) != cudaSuccess)
+    return alloc_fail();
+  {
+    int rc = ph_boruvka_mst(si, sj, E, n, mask, comp, ncomp, st + 1, mst_ws, mst_b, s);
+    if (rc == PH_OK) rc = ph_h0_rows(filt, mask, E, n, res->rows[0], h0_ws, h0_b, s);
+    if (rc != PH_OK) return give_up(rc);
+  }
+  res->nrows[0] = n;
+  if (max_dim == 0) {
+    const int64_t* src[1] = {cnt + 1};
+    if (readback(src, 1, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int st_mst = (int)(H[0] >> 32);
+    if (st_mst) return give_up(fail(st_mst, "ph_boruvka_mst failed"));
+    *out = res;
+    return PH_OK;
+  }
+
+  // ---- 4. triangles (triangle_kernel.py:288; reduce_h1_gpu.py:65-100) -------------------------
+  int64_t* tri_off = A.take<int64_t>(E + 1);
+  int64_t* tcof_off = A.take<int64_t>(E + 1);
+  const size_t tc_b = ph_triangles_count_workspace_bytes(E);
+  void* tc_ws = A.bytes(tc_b);
+  if (A.failed) return alloc_fail();
+  {
+    int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
+    if (rc != PH_OK) return give_up(rc);
+    const int64_t* src[2] = {tri_off + E, cnt + 1};
+    if (readback(src, 2, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+  }
+  const i64 T = H[0];
+  if ((int)(H[1] >> 32) != 0) return give_up(fail((int)(H[1] >> 32), "ph_boruvka_mst failed"));
+  if (T > max_triangles) {
+    char m[200];
+    snprintf(m, sizeof m,
+             "Triangle count %lld exceeds max_triangles=%lld. Reduce max_edge_length or increase max_triangles.",
+             (long long)T, (long long)max_triangles);
+    return give_up(fail(PH_ERR_LIMIT, m));
+  }
+  if (E + 3 * T >= (int64_t(1) << 31)) {
+    char m[120];
+    snprintf(m, sizeof m, "Triangle count %lld exceeds the int32 rank range", (long long)T);
+    return give_up(fail(PH_ERR_LIMIT, m));
+  }
+  res->stats[1] = T;
+  i32* tri_m = A.take<i32>(T);
+  i32* tri_w = A.take<i32>(T);
+  i32* tri_fa = A.take<i32>(T);
+  i32* tri_fb = A.take<i32>(T);
+  i32* off1 = A.take<i32>(E + 1);
+  i32* data1 = A.take<i32>(3 * T);
+  i32* cmf1 = A.take<i32>(T);
+  const size_t cc_b = ph_cofacet_csr_workspace_bytes(T, 3);
+  void* cc_ws = A.bytes(cc_b);
+  if (A.failed || cudaMallocAsync((void**)&res->rows[1], sizeof(float) * 2 * std::max<i64>(E, 1), s) != cudaSuccess)
+    return alloc_fail();
+  if (T) {
+    int rc = ph_triangles_emit(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tri_m, tri_w, tri_fa, tri_fb, s);
+    if (rc == PH_OK)
+      rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
+    if (rc == PH_OK) rc = ph_cof_max_face(nullptr, tri_m, tri_fa, tri_fb, 3, T, 0, mask, cmf1, s);
+    if (rc != PH_OK) return give_up(rc);
+  } else {
+    cudaMemsetAsync(off1, 0, sizeof(i32) * (E + 1), s);
+  }
+
+  // ---- 5. H1 reduction and rows (reduce_h1_gpu.py:159-223, 574-604) --------------------------
+  i64 pool1 = std::max<i64>(16 * (3 * T) + 2 * E, 1 << 22);
+  RedOut r1{};
+  int64_t* tet_off = nullptr;
+  void* tq_ws = nullptr;
+  size_t tq_b = 0;
+  if (max_dim == 2) {
+    tet_off = A.take<int64_t>(E + 1);
+    tq_b = ph_tets_count_workspace_bytes(E);
+    tq_ws = A.bytes(tq_b);
+    if (A.failed) return alloc_fail();
+  }
+  for (int attempt = 0;; ++attempt) {
+    int rc = reduce_rows(A, s, off1, data1, E, 0, T, (i32)E, mask, cmf1, filt, nullptr, tri_m, pool1, st + 2,
+                         res->rows[1], r1);
+    if (rc != PH_OK) return give_up(rc);
+    if (max_dim == 2 && attempt == 0) {
+      // the tetrahedron count only needs the triangles: launch it before waiting
+      rc = ph_tets_count(tri_off, tri_w, E, adj_ptr, adj_idx, adj_rank, nullptr, tet_off, tq_ws, tq_b, s);
+      if (rc != PH_OK) return give_up(rc);
+    }
+    const int64_t* src[4] = {cnt + 2, r1.nrows, r1.info + 1, max_dim == 2 ? tet_off + E : r1.nrows};
+    if (readback(src, 4, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int st_red = (int)(H[0] & 0xffffffff);
+    if (st_red == PH_OK) break;
+    if (st_red != PH_ERR_POOL || attempt >= 3) return give_up(fail(st_red, "ph_reduce (H1) failed"));
+    pool1 *= 4;
+    cudaMemsetAsync(st + 2, 0, sizeof(int), s);
+  }
+  res->nrows[1] = H[1];
+  res->stats[3] = H[2];
+  if (max_dim == 1) {
+    *out = res;
+    return PH_OK;
+  }
+
+  // ---- 6. H2 (triangle_kernel.py:402; cohomology_general.py) --------------------------------
+  const i64 Q = H[3];
+  if (Q > max_tetrahedra) {
+    char m[200];
+    snprintf(m, sizeof m,
+             "Tetrahedra count %lld exceeds max_tetrahedra=%lld. Reduce max_edge_length or increase max_tetrahedra.",
+             (long long)Q, (long long)max_tetrahedra);
+    return give_up(fail(PH_ERR_LIMIT, m));
+  }
+  if (E + T + Q >= (int64_t(1) << 31) || 4 * Q >= (int64_t(1) << 31)) {
+    char m[120];
+    snprintf(m, sizeof m, "Tetrahedra count %lld exceeds the int32 rank range", (long long)Q);
+    return give_up(fail(PH_ERR_LIMIT, m));
+  }
+  res->stats[2] = Q;
+  i32* tet_m = A.take<i32>(Q);
+  i32* tet_faces = A.take<i32>(4 * Q);
+  uint8_t* skip2 = A.take<uint8_t>(T);
+  i32* cmf2 = A.take<i32>(Q);
+  i32* off2 = A.take<i32>(T + 1);
+  i32* data2 = A.take<i32>(4 * Q);
+  const size_t c2_b = ph_cofacet_csr_workspace_bytes(Q, 4);
+  void* c2_ws = A.bytes(c2_b);
+  if (A.failed || cudaMallocAsync((void**)&res->rows[2], sizeof(float) * 2 * std::max<i64>(T, 1), s) != cudaSuccess)
+    return alloc_fail();
+  {
+    int rc = PH_OK;
+    if (Q)
+      rc = ph_tets_emit(si, sj, E, tri_off, tri_w, tri_fa, tri_fb, adj_ptr, adj_idx, adj_rank, nullptr, tet_off,
+                        tet_m, tet_faces, st + 3, s);
+    if (rc == PH_OK) rc = ph_mark_pivots(r1.state, r1.piv, E, (i32)E, skip2, T, s);
+    if (rc == PH_OK && Q) rc = ph_cof_max_face(tet_faces, nullptr, nullptr, nullptr, 4, Q, (i32)E, skip2, cmf2, s);
+    if (rc == PH_OK && Q)
+      rc = ph_cofacet_csr(tet_faces, nullptr, nullptr, nullptr, 4, Q, T, (i32)(E + T), off2, data2, c2_ws, c2_b, s);
+    if (rc != PH_OK) return give_up(rc);
+    if (!Q) cudaMemsetAsync(off2, 0, sizeof(i32) * (T + 1), s);
+  }
+  i64 pool2 = std::max<i64>(16 * (4 * Q) + 2 * T, 1 << 22);
+  RedOut r2{};
+  for (int attempt = 0;; ++attempt) {
+    int rc = reduce_rows(A, s, off2, data2, T, (i32)E, Q, (i32)(E + T), skip2, cmf2, filt, tri_m, tet_m, pool2,
+                         st + 4, res->rows[2], r2);
+    if (rc != PH_OK) return give_up(rc);
+    const int64_t* src[4] = {cnt + 2, cnt + 3, r2.nrows, r2.info + 1};
+    if (readback(src, 4, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int st_emit = (int)(H[0] >> 32), st_red = (int)(H[1] & 0xffffffff);
+    if (st_emit) return give_up(fail(st_emit, "ph_tets_emit failed"));
+    if (st_red == PH_OK) break;
+    if (st_red != PH_ERR_POOL || attempt >= 3) return give_up(fail(st_red, "ph_reduce (H2) failed"));
+    pool2 *= 4;
+    cudaMemsetAsync(st + 4, 0, sizeof(int), s);
+  }
+  res->nrows[2] = H[2];
+  res->stats[4] = H[3];
+  *out = res;
+  return PH_OK;
+}
+
+extern "C" int64_t ph_result_rows(const ph_result* r, int32_t dim) {
+  if (!r || dim < 0 || dim >= r->ndim) return -1;
+  return r->nrows[dim];
+}
+
+extern "C" int64_t ph_result_stat(const ph_result* r, int32_t k) {
+  if (!r || k < 0 || k >= 8) return -1;
+  return r->stats[k];
+}
+
+extern "C" int ph_result_copy(const ph_result* r, int32_t dim, float* dst, int32_t to_host, void* stream) {
+  if (!r || dim < 0 || dim >= r->ndim || (!dst && r->nrows[dim])) return PH_ERR_ARG;
+  if (!r->nrows[dim]) return PH_OK;
+  const cudaError_t e = cudaMemcpyAsync(dst, r->rows[dim], sizeof(float) * 2 * r->nrows[dim],
+                                        to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                        (cudaStream_t)stream);
+  if (e != cudaSuccess) {
+    record_error(e);
+    return PH_ERR_CUDA;
+  }
+  return PH_OK;
+}
+
+extern "C" void ph_result_free(ph_result* r) {
+  if (!r) return;
+  for (float* p : r->rows)
+    if (p) cudaFreeAsync(p, r->stream);
+  delete r;
+}

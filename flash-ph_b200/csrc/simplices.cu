@@ -238,10 +238,11 @@ extern "C" int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, 
   i32* cc = c.take<i32>(E + 1);
   void* sws = c.take<char>((i64)scan_workspace_bytes(E));
   if (!tc || !cc || !sws) return PH_ERR_ARG;
-  if (E > 0)
+  if (E > 0) {
     ph::count_launch();
     k_triangles<false><<<warp_grid(E), SX_NT, 0, s>>>(edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, tc, cc,
                                                       nullptr, nullptr, nullptr, nullptr, nullptr);
+  }
   PH_TRY(scan_exclusive_i32_i64(tc, tri_off, E, sws, scan_workspace_bytes(E), s));
   PH_TRY(scan_exclusive_i32_i64(cc, cof_off, E, sws, scan_workspace_bytes(E), s));
   PH_CHECK_LAUNCH();
@@ -274,11 +275,12 @@ extern "C" int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64
   i32* qc = c.take<i32>(E + 1);
   void* sws = c.take<char>((i64)scan_workspace_bytes(E));
   if (!qc || !sws) return PH_ERR_ARG;
-  if (E > 0)
+  if (E > 0) {
     ph::count_launch();
     k_tets<false><<<warp_grid(E), SX_NT, 0, s>>>(nullptr, nullptr, E, tri_off, tri_w, nullptr, nullptr, adj_ptr,
                                                  adj_idx, adj_rank, edge_enable, qc, nullptr, nullptr, nullptr,
                                                  nullptr);
+  }
   PH_TRY(scan_exclusive_i32_i64(qc, tet_off, E, sws, scan_workspace_bytes(E), s));
   PH_CHECK_LAUNCH();
   return PH_OK;

@@ -17,7 +17,8 @@ _LIB = None
 
 PH_OK = 0
 _STATUS = {1: "CUDA error", 2: "invalid argument", 3: "capacity exceeded",
-           4: "iteration limit reached", 5: "reduction pool exhausted", 6: "count overflow"}
+           4: "iteration limit reached", 5: "reduction pool exhausted", 6: "count overflow",
+           7: "limit exceeded"}
 
 P = ctypes.c_void_p
 I64 = ctypes.c_int64
@@ -50,6 +51,12 @@ _SIGS = {
     "ph_tets_count": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, SZ, P]),
     "ph_tets_emit": (ctypes.c_int, [P, P, I64, P, P, P, P, P, P, P, P, P, P, P, P, P]),
     "ph_cloud_tiles": (I64, [I64]),
+    "ph_rips_persistence": (ctypes.c_int, [P, I64, I32, ctypes.c_double, I32, I64, I64, I32,
+                                           ctypes.POINTER(ctypes.c_void_p), P]),
+    "ph_result_rows": (I64, [P, I32]),
+    "ph_result_stat": (I64, [P, I32]),
+    "ph_result_copy": (ctypes.c_int, [P, I32, P, I32, P]),
+    "ph_result_free": (None, [P]),
     "ph_edges_screened_workspace_bytes": (SZ, [I64, I32, I32]),
     "ph_batch_edges_enumerate_screened": (ctypes.c_int, [P, P, I32, I64, I32, I64, P, I64, P, P, P, I64, P, P, P,
                                                          P, SZ, P]),

@@ -9,10 +9,14 @@ device and the results are returned on the input's device.
 """
 from __future__ import annotations
 
+import ctypes
+import os
+
 import numpy as np
 import torch
 from torch import Tensor
 
+from . import _lib as L
 from . import _timing
 from ._lib import check_status
 from .boruvka import boruvka_mask, h0_rows
@@ -80,16 +84,64 @@ def rips_persistence(
     if points.device.type != "cuda":
         if not torch.cuda.is_available():
             raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
-        points = points.cuda()
+        points = points.cuda(non_blocking=points.is_pinned())
     dev = points.device
     with torch.cuda.device(dev):
-        dgms = _compute(points, float(max_edge_length), max_dim)
+        if os.environ.get("FLASHPH_PIPELINE", "native") == "staged":
+            dgms = _compute_staged(points, float(max_edge_length), max_dim)
+        else:
+            return _compute_native(points.float().contiguous(), float(max_edge_length), max_dim, out_device)
     if out_device != dev:
         dgms = [d.to(out_device) for d in dgms]
     return dgms
 
 
-def _compute(points: Tensor, t: float, max_dim: int) -> list[Tensor]:
+_EDGE_MODES = {"auto": 0, "on": 1, "off": 2}
+
+
+def _compute_native(points: Tensor, t: float, max_dim: int, out_device, max_triangles: int = 10_000_000,
+                    max_tetrahedra: int = 10_000_000) -> list[Tensor]:
+    """The whole call in the CUDA library (ph_rips_persistence); diagrams are
+    copied straight to the caller's device (pinned host memory for CPU
+    callers)."""
+    n, d = points.shape
+    dev = points.device
+    mode = _EDGE_MODES.get(os.environ.get("FLASHPH_EDGE_SCREEN", "auto").lower(), 0)
+    if mode == 1 and d > 252:
+        mode = 2
+    s = L.stream_handle(dev)
+    res = ctypes.c_void_p()
+    lib = L.lib()
+    with _timing.stage("native"):
+        rc = lib.ph_rips_persistence(points.data_ptr(), n, d, t, max_dim, max_triangles, max_tetrahedra, mode,
+                                     ctypes.byref(res), s)
+    if rc != L.PH_OK:
+        msg = lib.ph_last_error().decode(errors="replace")
+        if rc == 7:  # PH_ERR_LIMIT: the reference raises ValueError with this text
+            raise ValueError(msg)
+        raise L.PHError("ph_rips_persistence", rc, msg)
+    try:
+        to_host = out_device.type != "cuda"
+        outs = []
+        for k in range(max_dim + 1):
+            m = int(lib.ph_result_rows(res, k))
+            if to_host:
+                o = torch.empty(m, 2, dtype=torch.float32, pin_memory=True)
+            else:
+                o = torch.empty(m, 2, dtype=torch.float32, device=out_device)
+            L.call("ph_result_copy", res, k, o.data_ptr(), 1 if to_host else 0, s)
+            outs.append(o)
+        if to_host:
+            torch.cuda.current_stream(dev).synchronize()
+    finally:
+        lib.ph_result_free(res)
+    return outs
+
+
+def _compute_staged(points: Tensor, t: float, max_dim: int) -> list[Tensor]:
+    """The same computation stage by stage from Python (each stage its own
+    library call); kept as a cross-check of the native pipeline and for the
+    stage-level timers."""
     n = points.shape[0]
     with _timing.stage("filtration"):
         filt = rips_filtration(points, t)

@@ -33,6 +33,7 @@ extern "C" {
 #define PH_ERR_ITER_LIMIT 4  /* a bounded device loop hit its iteration cap  */
 #define PH_ERR_POOL 5        /* reduction column pool exhausted              */
 #define PH_ERR_OVERFLOW 6    /* a count does not fit the index type          */
+#define PH_ERR_LIMIT 7       /* a user limit was exceeded (ValueError text)  */
 
 /* Library version (major*10000 + minor*100 + patch). */
 int ph_version(void);
@@ -271,6 +272,31 @@ int ph_persistence_rows(const int32_t* col_state, const int32_t* col_piv, int64_
                         int32_t row_base, const float* filt, const int32_t* col_m,
                         const int32_t* row_m, float* out_rows, int64_t* d_nrows, void* workspace,
                         size_t workspace_bytes, void* stream);
+
+/* ---- the whole call --------------------------------------------------------- */
+
+/* rips_persistence for one cloud, every stage on `stream`: points (device,
+ * n x d float32, n >= 2), max_edge_length (edges keep dist^2 <
+ * fp32(max_edge_length^2)), max_dim 0..2, the reference's max_triangles /
+ * max_tetrahedra limits, edge_mode 0 (tensor-core screen when 8 <= d <= 252),
+ * 1 (screen), 2 (direct kernel). On success *out holds the diagrams on the
+ * device; read them with ph_result_rows / ph_result_copy and release with
+ * ph_result_free. A limit exceeded returns PH_ERR_LIMIT with the reference's
+ * ValueError message in ph_last_error(). The host waits at most four times
+ * (edge, triangle and tetrahedron counts, reduction statuses).
+ * Replaces persistence.py:77-215 rips_persistence (the n >= 2 path). */
+typedef struct ph_result ph_result;
+int ph_rips_persistence(const float* points, int64_t n, int32_t d, double max_edge_length, int32_t max_dim,
+                        int64_t max_triangles, int64_t max_tetrahedra, int32_t edge_mode, ph_result** out,
+                        void* stream);
+/* rows of diagram dim (0..max_dim), -1 if out of range */
+int64_t ph_result_rows(const ph_result* result, int32_t dim);
+/* run statistics: 0 edges, 1 triangles, 2 tetrahedra, 3 H1 column additions,
+ * 4 H2 column additions */
+int64_t ph_result_stat(const ph_result* result, int32_t k);
+/* copies diagram dim (rows x 2 float32) to dst, device or host memory */
+int ph_result_copy(const ph_result* result, int32_t dim, float* dst, int32_t to_host, void* stream);
+void ph_result_free(ph_result* result);
 
 /* ---- batches of clouds ---------------------------------------------------- */
 

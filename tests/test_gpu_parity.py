@@ -190,3 +190,33 @@ def test_twenty_k_matches_oracle():
     assert _same_rows(dg[0].cpu().numpy(), ref["h0"])
     assert _same_rows(dg[1].cpu().numpy(), ref["h1"])
     assert _same_rows(sorted_rows(dg[2].cpu().numpy()), sorted_rows(ref["h2"]))
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_native_pipeline_equals_staged(name, monkeypatch):
+    """ph_rips_persistence (one native call) and the stage-by-stage Python
+    path give the same diagrams, bit for bit and in the same row order."""
+    from flashph_b200 import rips_persistence
+    z, meta = load_golden(name)
+    pts, t, md = z["points"], float(z["t"]), meta["max_dim"]
+    native = rips_persistence(_fp(pts), t, max_dim=md)
+    monkeypatch.setenv("FLASHPH_PIPELINE", "staged")
+    staged = rips_persistence(_fp(pts), t, max_dim=md)
+    assert len(native) == len(staged)
+    for a, b in zip(native, staged):
+        assert _bits(a.cpu().numpy()).shape == _bits(b.cpu().numpy()).shape
+        assert np.array_equal(_bits(a.cpu().numpy()), _bits(b.cpu().numpy()))
+
+
+def test_native_pipeline_host_arrays_and_limits():
+    from flashph_b200 import rips_persistence
+    rng = np.random.default_rng(21)
+    pts = rng.standard_normal((3000, 10)).astype(np.float32)
+    dev = rips_persistence(torch.from_numpy(pts).cuda(), 1.6, max_dim=2)
+    host = rips_persistence(torch.from_numpy(pts), 1.6, max_dim=2)  # CPU in, CPU out
+    for a, b in zip(dev, host):
+        assert b.device.type == "cpu"
+        assert np.array_equal(_bits(a.cpu().numpy()), _bits(b.numpy()))
+    dense = rng.standard_normal((400, 3)).astype(np.float32)  # complete graph: C(400, 3) > 10^7 triangles
+    with pytest.raises(ValueError, match="exceeds max_triangles=10000000"):
+        rips_persistence(torch.from_numpy(dense).cuda(), 100.0, max_dim=1)
