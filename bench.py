@@ -424,6 +424,11 @@ def run_precision(args, rank, local):
                       "identical_to_direct": identical, "screen_candidates": stats["candidates"],
                       "forced_pairs": stats["forced"],
                       "candidates_per_edge": round(stats["candidates"] / max(1, int(ka.shape[0])), 3)},
+            "roofline": {"kernel": "k_tc_edges (tensor-core screened edge enumeration, with its prep kernels)",
+                         "bound": "tensor", "achieved": round(tc_flops / (scr_ms * 1e-3) / 1e12, 2),
+                         "peak": bf16_peak, "unit": "TFLOP/s",
+                         "frac": round(tc_flops / (scr_ms * 1e-3) / 1e12 / bf16_peak, 4), "traffic": None,
+                         "algorithmic_flops_per_launch": tc_flops, "avg_launch_ms": round(scr_ms, 4)},
             "tensor": {"mma_flops": tc_flops, "tflops": round(tc_flops / (scr_ms * 1e-3) / 1e12, 2),
                        "peak_bf16_tflops": bf16_peak, "frac": round(tc_flops / (scr_ms * 1e-3) / 1e12 / bf16_peak, 4),
                        "peak_source": src},
@@ -431,6 +436,112 @@ def run_precision(args, rank, local):
             "fp64_error": errs,
             "rows": [int(o.shape[0]) for o in out],
             "cpu_baseline": cpu, "clocks": clocks.summary()}), flush=True)
+
+
+def kernel_breakdown(pts, t, max_dim, flush, reps=3):
+    """Per-stage device times of the staged pipeline (CUDA events around each
+    stage's launches) and of the screened edge kernel alone, plus the sizes
+    the algorithmic byte and flop counts need. Runs outside the timed region."""
+    import torch
+    from flashph_b200 import _timing, rips_persistence
+    from flashph_b200.cohomology import enumerate_triangles
+    from flashph_b200.rips import enumerate_edges, rips_filtration
+
+    os.environ["FLASHPH_PIPELINE"] = "staged"
+    try:
+        rips_persistence(pts, t, max_dim=max_dim)
+        with _timing.record() as ev:
+            for _ in range(reps):
+                flush.zero_()
+                rips_persistence(pts, t, max_dim=max_dim)
+            torch.cuda.synchronize()
+        st = _timing.summarize(ev)
+    finally:
+        os.environ.pop("FLASHPH_PIPELINE", None)
+    stages = {k: v[1] / max(v[0], 1) for k, v in st.items()}
+    # the screened edge launches alone (as ph_rips_persistence makes them),
+    # buffers prepared once, no host read-back inside the events
+    import numpy as np
+    from flashph_b200 import _lib as L
+    from flashph_b200.rips import _SEG_DTYPE, threshold_sq
+    n, d = pts.shape
+    seg = np.zeros(1, dtype=_SEG_DTYPE)
+    seg[0] = (0, 0, 0, n, d, threshold_sq(t), 1)
+    segd = torch.from_numpy(seg.view(np.uint8).copy()).to(pts.device)
+    nb = (n + 127) // 128
+    blk = torch.tensor([0, nb], dtype=torch.int64, device=pts.device)
+    cap = max(int(enumerate_edges(pts, t, screen=True)[0].shape[0]), 1)
+    ei = torch.empty(cap, dtype=torch.int32, device=pts.device)
+    ej, ed = torch.empty_like(ei), torch.empty(cap, dtype=torch.float32, device=pts.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=pts.device)
+    stt = torch.zeros(1, dtype=torch.int32, device=pts.device)
+    wsb = L.query("ph_edges_screened_workspace_bytes", n, 1, d)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=pts.device)
+    ntiles = L.query("ph_cloud_tiles", n)
+    ts = []
+    for _ in range(reps + 3):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        L.call("ph_batch_edges_enumerate_screened", pts.data_ptr(), segd.data_ptr(), 1, ntiles, d, n,
+               blk.data_ptr(), nb, ei.data_ptr(), ej.data_ptr(), ed.data_ptr(), cap, cnt.data_ptr(),
+               stt.data_ptr(), 0, ws.data_ptr(), wsb, L.stream_handle(pts.device))
+        b.record()
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    edge_ms = statistics.median(ts[2:])
+    filt = rips_filtration(pts, t)
+    E = int(filt.edge_i.shape[0])
+    T = enumerate_triangles(filt).T if max_dim >= 1 else 0
+    return stages, edge_ms, E, T
+
+
+# DRAM traffic per launch from ncu captures of this workload (profiles/*.md)
+NCU_TRAFFIC = {
+    "k_tc_edges": {"bytes": 2.29e6 + 0.02e6, "source": "profiles/k_tc_edges_20k_d10.md"},
+    "k_reduce": {"bytes": 0.87e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
+}
+
+
+def rooflines(stages, edge_ms, n, d, E, T, pk, src):
+    """Roofline entries of the three kernels that dominate the call."""
+    nt = (n + 127) // 128
+    ks = (d + 4 + 15) // 16
+    mma_flops = 2.0 * 128 * 128 * 16 * ks * nt * (nt + 1) / 2
+    tf = mma_flops / (edge_ms * 1e-3) / 1e12
+    bf16 = pk.get("bf16_tflops", 1590.0)
+    hbm = pk.get("hbm_gbs", 6650.0)
+    out = {}
+    out["edges"] = {"kernel": "k_tc_edges (tensor-core screened edge enumeration, with its 4 prep launches)",
+                    "bound": "tensor", "achieved": round(tf, 2), "peak": bf16, "unit": "TFLOP/s",
+                    "frac": round(tf / bf16, 4), "traffic": NCU_TRAFFIC["k_tc_edges"]["bytes"],
+                    "traffic_source": NCU_TRAFFIC["k_tc_edges"]["source"],
+                    "algorithmic_flops_per_launch": mma_flops, "avg_launch_ms": round(edge_ms, 5),
+                    "per_unit": "2 x 128 x 128 x 16*ceil((d+4)/16) MMA flops per 128x128 point tile, "
+                                "nt(nt+1)/2 tiles", "peak_source": f"bf16_tflops burst ({src} peaks file)"}
+    if "sort" in stages:
+        byts = 2.0 * 12 * E
+        gbs = byts / (stages["sort"] * 1e-3) / 1e9
+        out["sort"] = {"kernel": "filtration sort (k_os_hist, 8 x k_os_pass, k_os_finish)", "bound": "hbm",
+                       "achieved": round(gbs, 2), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 5),
+                       "traffic": None, "algorithmic_bytes_per_launch": byts,
+                       "avg_launch_ms": round(stages["sort"], 5),
+                       "per_unit": "12 bytes (i, j, dist^2) read and written per edge",
+                       "peak_source": f"hbm_gbs ({src} peaks file)"}
+    if "h1.reduce" in stages:
+        byts = 4.0 * (E + 1) + 4.0 * 3 * T + 4.0 * T + 1.0 * E + 8.0 * E + 8.0 * T
+        gbs = byts / (stages["h1.reduce"] * 1e-3) / 1e9
+        out["h1.reduce"] = {"kernel": "k_reduce (H1, with classify/finish/rows)", "bound": "hbm",
+                            "achieved": round(gbs, 3), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 6),
+                            "traffic": NCU_TRAFFIC["k_reduce"]["bytes"],
+                            "traffic_source": NCU_TRAFFIC["k_reduce"]["source"],
+                            "algorithmic_bytes_per_launch": byts, "avg_launch_ms": round(stages["h1.reduce"], 5),
+                            "per_unit": "cofacet CSR (4 B per offset and entry), cmf 4 B and owner word 8 B per "
+                                        "triangle, mask 1 B and state/pivot 8 B per edge",
+                            "note": "latency-bound: the reduction is a chain of dependent column additions "
+                                    "(the oracle's critical path), not a bandwidth problem",
+                            "peak_source": f"hbm_gbs ({src} peaks file)"}
+    return out
 
 
 def dist_setup():
@@ -546,8 +657,6 @@ def main():
     per = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms = statistics.mean(per)
     st = _timing.summarize(stages)
-    edge_cnt, edge_ms = st.get("edges", (1, float("nan")))
-    edge_ms /= max(edge_cnt, 1)
 
     # end to end through the public API with host buffers
     e2e_ms = []
@@ -565,17 +674,19 @@ def main():
         d2h = sum(r.numel() * 4 for r in res)
     e2e = statistics.mean(e2e_ms)
 
-    vals = torch.tensor([ms, e2e, edge_ms], dtype=torch.float64, device=dev)
+    vals = torch.tensor([ms, e2e], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, e2e, edge_ms = (float(x) for x in vals.cpu())
+    ms, e2e = (float(x) for x in vals.cpu())
 
     if rank == 0:
         pk, src = peaks()
         cs = clocks.summary()
-        flops = 3.0 * DIM * N_POINTS * (N_POINTS - 1) / 2.0
-        fp32_peak = 148 * 128 * 2 * (pk.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
-        achieved = flops / (edge_ms * 1e-3) / 1e12
+        stage_ms, edge_ms, E, T = kernel_breakdown(pts, THRESH, MAX_DIM, flush)
+        rl = rooflines(stage_ms, edge_ms, N_POINTS, DIM, E, T, pk, src)
+        leaf = {k: v for k, v in stage_ms.items() if k in ("edges", "sort", "vertex_csr", "h1.triangles",
+                                                           "h1.cofacets", "h1.reduce", "h2")}
+        dominant = max(leaf, key=leaf.get) if leaf else "edges"
         cpu = None
         if not args.no_cpu_baseline:
             import oracle
@@ -599,14 +710,15 @@ def main():
             "e2e": {"value": round(e2e, 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "k_edges (edge enumeration)", "bound": "fp32-alu",
-                         "achieved": round(achieved, 3), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
-                         "frac": round(achieved / fp32_peak, 4), "traffic": None,
-                         "algorithmic_flops_per_launch": flops, "avg_launch_ms": round(edge_ms, 5),
-                         "peak_source": f"148 SMs x 128 FP32 lanes x 2 x sm_max_mhz ({src} peaks file)"},
+            "roofline": dict(rl.get(dominant, rl["edges"]), stage=dominant),
+            "rooflines": rl,
             "cpu_baseline": cpu,
             "clocks": cs,
-            "stages_ms": {k: round(v[1] / max(v[0], 1), 4) for k, v in st.items()},
+            "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "stages_source": "staged pipeline (the same stages called one by one from Python), CUDA events "
+                             "around each stage, 3 calls outside the timed region; the timed calls run the "
+                             "native pipeline",
+            "sizes": {"edges": E, "triangles": T},
         }
         if not args.no_serving:
             line["serving"] = serving_summary(args.serving_requests, rates_rel=(0.5,))
