@@ -481,8 +481,7 @@ extern "C" int ph_batch_knn_kth(const float* pts, const ph_cloud_seg* segs, int3
   if (nqb == 0) return PH_OK;
   const size_t smem = sizeof(float) * ((size_t)max_d * KN_NT + (size_t)KN_TP * max_d);
   if (smem > 200 * 1024) return PH_ERR_ARG;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_knn_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_knn_batch);
   ph::count_launch();
   k_knn_batch<<<(unsigned)nqb, KN_NT, smem, (cudaStream_t)stream>>>(pts, segs, nsegs, qb_off, k, out);
   PH_CHECK_LAUNCH();

@@ -37,6 +37,12 @@ void record_message(const char* msg);
 // Counts kernel launches made by this library (reported by ph_launch_count()).
 void count_launch();
 
+// Raises a kernel's dynamic shared memory limit to the device's opt-in
+// maximum (minus the kernel's static shared memory). Always the same value,
+// so threads launching the kernel concurrently with different requests
+// cannot lower each other's limit. Returns cudaSuccess or the error.
+cudaError_t allow_dynamic_smem(const void* func);
+
 }  // namespace ph
 
 #define PH_CHECK_LAUNCH()                         \

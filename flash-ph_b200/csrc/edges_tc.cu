@@ -885,7 +885,7 @@ extern "C" int ph_batch_edges_enumerate_screened(const float* pts, const ph_clou
     record_message("ph_batch_edges_enumerate_screened: tensor map encoding failed");
     return PH_ERR_CUDA;
   }
-  if (cudaFuncSetAttribute(k_tc_edges, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem) != cudaSuccess) {
+  if (ph::allow_dynamic_smem((const void*)k_tc_edges) != cudaSuccess) {
     PH_CHECK_LAUNCH();
     return PH_ERR_CUDA;
   }

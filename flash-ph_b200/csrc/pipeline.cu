@@ -124,6 +124,14 @@ int readback(const int64_t* const* src, int count, int64_t* dst, cudaStream_t s)
   return PH_OK;
 }
 
+// reduction pool (int32 entries): initial records (at most 2 nnz), per-warp
+// chunks, reduced columns; bounded by the 33-bit record offsets
+constexpr i64 POOL_MAX = (i64(1) << 33) - 1;
+i64 pool_capacity(i64 nnz, i64 K) {
+  const i64 mult = nnz < (i64(1) << 24) ? 8 : 3;
+  return std::min<i64>(mult * nnz + 2 * K + (i64(1) << 23), POOL_MAX);
+}
+
 struct RedOut {
   i32* state;
   i32* piv;
@@ -187,7 +195,8 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   ph_cloud_seg* seg = A.take<ph_cloud_seg>(1);
   int64_t* blk = A.take<int64_t>(2);
   // cnt[0]: edge count; statuses as int32 words from cnt + 1: st[0] edges,
-  // st[1] forest, st[2] H1 reduction, st[3] tetrahedra, st[4] H2 reduction
+  // st[1] forest, st[2] H1 reduction, st[3] tetrahedra, st[4] H2 reduction;
+  // cnt[5] triangle total, cnt[6] its work counter
   int64_t* cnt = A.take<int64_t>(8);
   if (A.failed) return alloc_fail();
   cudaMemsetAsync(cnt, 0, 8 * sizeof(int64_t), s);
@@ -281,7 +290,18 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   const size_t tc_b = ph_triangles_count_workspace_bytes(E);
   void* tc_ws = A.bytes(tc_b);
   if (A.failed) return alloc_fail();
-  {
+  // On dense graphs the per-edge count costs sum(deg^2); the exact total comes
+  // first from a cheaper rank-free pass, so that a call over the triangle
+  // limit fails without the per-edge pass.
+  const bool total_first =
+      4.0 * (double)E * (double)E / (double)n > 2e8 && n <= ph_triangles_total_max_vertices();
+  if (total_first) {
+    int rc = ph_triangles_total(adj_ptr, adj_idx, n, reinterpret_cast<unsigned long long*>(cnt + 5),
+                                reinterpret_cast<int*>(cnt + 6), s);
+    if (rc != PH_OK) return give_up(rc);
+    const int64_t* src[2] = {cnt + 5, cnt + 1};
+    if (readback(src, 2, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+  } else {
     int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[2] = {tri_off + E, cnt + 1};
@@ -302,6 +322,10 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     return give_up(fail(PH_ERR_LIMIT, m));
   }
   res->stats[1] = T;
+  if (total_first) {  // per-edge counts for the emission offsets (their sum is T)
+    int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
+    if (rc != PH_OK) return give_up(rc);
+  }
   i32* tri_m = A.take<i32>(T);
   i32* tri_w = A.take<i32>(T);
   i32* tri_fa = A.take<i32>(T);
@@ -324,7 +348,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   }
 
   // ---- 5. H1 reduction and rows (reduce_h1_gpu.py:159-223, 574-604) --------------------------
-  i64 pool1 = std::max<i64>(16 * (3 * T) + 2 * E, 1 << 22);
+  i64 pool1 = pool_capacity(3 * T, E);
   RedOut r1{};
   int64_t* tet_off = nullptr;
   void* tq_ws = nullptr;
@@ -348,8 +372,9 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (readback(src, 4, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_red = (int)(H[0] & 0xffffffff);
     if (st_red == PH_OK) break;
-    if (st_red != PH_ERR_POOL || attempt >= 3) return give_up(fail(st_red, "ph_reduce (H1) failed"));
-    pool1 *= 4;
+    if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
+      return give_up(fail(st_red, "ph_reduce (H1) failed"));
+    pool1 = std::min<i64>(pool1 * 4, POOL_MAX);
     cudaMemsetAsync(st + 2, 0, sizeof(int), s);
   }
   res->nrows[1] = H[1];
@@ -396,7 +421,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (rc != PH_OK) return give_up(rc);
     if (!Q) cudaMemsetAsync(off2, 0, sizeof(i32) * (T + 1), s);
   }
-  i64 pool2 = std::max<i64>(16 * (4 * Q) + 2 * T, 1 << 22);
+  i64 pool2 = pool_capacity(4 * Q, T);
   RedOut r2{};
   for (int attempt = 0;; ++attempt) {
     int rc = reduce_rows(A, s, off2, data2, T, (i32)E, Q, (i32)(E + T), skip2, cmf2, filt, tri_m, tet_m, pool2,
@@ -407,8 +432,9 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     const int st_emit = (int)(H[0] >> 32), st_red = (int)(H[1] & 0xffffffff);
     if (st_emit) return give_up(fail(st_emit, "ph_tets_emit failed"));
     if (st_red == PH_OK) break;
-    if (st_red != PH_ERR_POOL || attempt >= 3) return give_up(fail(st_red, "ph_reduce (H2) failed"));
-    pool2 *= 4;
+    if (st_red != PH_ERR_POOL || attempt >= 3 || pool2 >= POOL_MAX)
+      return give_up(fail(st_red, "ph_reduce (H2) failed"));
+    pool2 = std::min<i64>(pool2 * 4, POOL_MAX);
     cudaMemsetAsync(st + 4, 0, sizeof(int), s);
   }
   res->nrows[2] = H[2];

@@ -392,12 +392,98 @@ __device__ __forceinline__ unsigned long long pool_alloc(PoolChunk& ch, RedCtl* 
   return __shfl_sync(FULL, at, 0);
 }
 
+// ---- dense working columns ---------------------------------------------------------
+// A working column longer than the shared buffer becomes a bitmap over the
+// row range in global memory, private to its warp (one slot per warp of the
+// grid, cleared on first use and after each column): adding a column flips
+// its bits, the next pivot is the first set bit at or after the current one
+// (the added column's entries are all >= the pivot it cancels), and the
+// sorted record is produced only when the column claims a pivot. Cost per
+// addition is the added column's length, not the working column's.
+struct DenseCol {
+  u32* bits = nullptr;  // this warp's slot
+  i64 lo = 0, hi = -1;  // touched word range
+  i32 piv = -1;         // lowest set bit (global rank)
+};
+
+// flips the sorted entries src[0..len) (global ranks); returns the change in
+// the number of set bits (warp-uniform) and widens the touched range
+__device__ int dense_flip(DenseCol& D, const i32* src, bool srcg, int len, i32 row_base) {
+  const int lane = threadIdx.x & 31;
+  int delta = 0;
+  for (int i = lane; i < len; i += 32) {
+    const i32 e = (srcg ? __ldcg(src + i) : src[i]) - row_base;
+    const u32 b = 1u << (e & 31);
+    const u32 old = atomicXor(D.bits + (e >> 5), b);
+    delta += (old & b) ? -1 : 1;
+  }
+  delta = __reduce_add_sync(FULL, delta);
+  if (len > 0) {
+    const i64 w0 = (i64)(((srcg ? __ldcg(src) : src[0]) - row_base) >> 5);
+    const i64 w1 = (i64)(((srcg ? __ldcg(src + len - 1) : src[len - 1]) - row_base) >> 5);
+    D.lo = D.hi < D.lo ? w0 : min(D.lo, w0);
+    D.hi = max(D.hi, w1);
+  }
+  __syncwarp();
+  return delta;
+}
+
+// first set bit at or after word `from` (global rank), -1 if none
+__device__ i32 dense_first(const DenseCol& D, i64 from, i32 row_base) {
+  const int lane = threadIdx.x & 31;
+  for (i64 w0 = from; w0 <= D.hi; w0 += 32) {
+    const i64 w = w0 + lane;
+    const u32 v = w <= D.hi ? __ldcg(D.bits + w) : 0u;
+    const u32 m = __ballot_sync(FULL, v != 0);
+    if (m) {
+      const int f = __ffs(m) - 1;
+      const u32 vw = __shfl_sync(FULL, v, f);
+      return (i32)(((w0 + f) << 5) + (__ffs(vw) - 1)) + row_base;
+    }
+  }
+  return -1;
+}
+
+// the set bits from the pivot's word on, ascending, into out[0..k)
+__device__ void dense_to_list(const DenseCol& D, i32 row_base, i32* out) {
+  const int lane = threadIdx.x & 31;
+  int pos = 0;
+  for (i64 w0 = (i64)((D.piv - row_base) >> 5); w0 <= D.hi; w0 += 32) {
+    const i64 w = w0 + lane;
+    u32 v = w <= D.hi ? __ldcg(D.bits + w) : 0u;
+    const int c = __popc(v);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int q = pos + incl - c;
+    while (v) {
+      out[q++] = (i32)((w << 5) + (__ffs(v) - 1)) + row_base;
+      v &= v - 1;
+    }
+    pos += __shfl_sync(FULL, incl, 31);
+  }
+  __syncwarp();
+}
+
+__device__ void dense_clear(DenseCol& D, i64 lo, i64 hi) {
+  const int lane = threadIdx.x & 31;
+  for (i64 w = lo + lane; w <= hi; w += 32) __stcg(D.bits + w, 0u);
+  __syncwarp();
+  D.lo = 0;
+  D.hi = -1;
+  D.piv = -1;
+}
+
 // Residual columns are taken in descending order (the serial algorithm's
 // order), RD_FETCH at a time per warp, so that a column mostly meets final
 // versions of the larger columns it adds and is rarely displaced.
 __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32* __restrict__ state,
                                                  const u64* __restrict__ rec, u64* owner, i32* pool, i64 pool_cap,
-                                                 int chunk, RedCtl* ctl, int* status, int max_steps) {
+                                                 int chunk, RedCtl* ctl, int* status, int max_steps,
+                                                 u32* dense_bits, i64 dense_words) {
   extern __shared__ i32 rd_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   i32* const sW0 = rd_smem + (size_t)w * RD_WSTRIDE;  // working copies at sW0 and sW0 + RD_CAP
@@ -405,6 +491,10 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
   volatile int* vabort = &ctl->abort;
   PoolChunk chunk_state;
   unsigned long long n_merges = 0, n_takeovers = 0;
+  DenseCol D;
+  bool dense_ready = false;  // this warp's slot has been cleared once
+  const bool dense_ok = dense_words > 0;
+  if (dense_ok) D.bits = dense_bits + (size_t)(blockIdx.x * RD_WARPS + w) * (size_t)dense_words;
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&ctl->next, RD_FETCH);
@@ -423,10 +513,26 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
     bool wg = false;      // W is in global memory
     bool published = false;
     u64 wrec = 0;         // record offset of W when published
+    bool dense = false;   // W is the bitmap D
+    auto enter_dense = [&](const i32* src, bool srcg, int len) {
+      if (!dense_ready) {
+        dense_clear(D, 0, dense_words - 1);
+        dense_ready = true;
+      }
+      dense_flip(D, src, srcg, len, row_base);
+      D.piv = srcg ? __ldcg(src) : src[0];
+      dense = true;
+    };
+    auto leave_dense = [&]() {
+      if (dense) dense_clear(D, D.lo, D.hi);
+      dense = false;
+    };
     auto load_record = [&](u64 at) {
       const i32* src = pool + at + 1;
       k = __ldcg(pool + at);
-      if (k <= RD_CAP) {
+      if (k > RD_CAP && dense_ok) {
+        enter_dense(src, true, k);
+      } else if (k <= RD_CAP) {
         for (int i = lane; i < k; i += 32) (sW0 + cur * RD_CAP)[i] = __ldcg(src + i);
         __syncwarp();
         W = (sW0 + cur * RD_CAP);
@@ -440,13 +546,14 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
     };
     load_record(rec[c]);
     for (int step = 0;; ++step) {
+      if (step > 0 && dense && *vabort) break;
       if (step >= max_steps) {
         if (lane == 0) set_status(status, PH_ERR_ITER_LIMIT);
         atomicExch(&ctl->abort, 1);
         break;
       }
       if (k == 0) break;  // the column vanished: it owns nothing
-      const i32 p = wg ? __ldcg(W) : W[0];
+      const i32 p = dense ? D.piv : (wg ? __ldcg(W) : W[0]);
       u64 ow = ld_acquire(owner + (p - row_base));
       i32 o = owner_col(ow);
       if (o < c) {
@@ -455,7 +562,10 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
           const unsigned long long at = pool_alloc(chunk_state, ctl, pool_cap, k + 1, chunk, status);
           if (at == ~0ull) break;
           if (lane == 0) pool[at] = k;
-          for (int i = lane; i < k; i += 32) pool[at + 1 + i] = wg ? __ldcg(W + i) : W[i];
+          if (dense)
+            dense_to_list(D, row_base, pool + at + 1);
+          else
+            for (int i = lane; i < k; i += 32) pool[at + 1 + i] = wg ? __ldcg(W + i) : W[i];
           wrec = at;
           published = true;
         }
@@ -466,6 +576,7 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
         __syncwarp();
         const i32 oc = owner_col(old);
         if (oc < c) {
+          leave_dense();
           if (oc < 0) break;  // claimed a free pivot: this work item is done
           // displaced a smaller column: take it over
           ++n_takeovers;
@@ -485,6 +596,18 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
       const i32 head = (at_o + lane < (u64)pool_cap) ? __ldcg(pool + at_o + lane) : 0;
       const int lb = __shfl_sync(FULL, head, 0);
       const i32 bv = __shfl_down_sync(FULL, head, 1);  // entry `lane` of B (lanes < 31)
+      if (!dense && dense_ok && k + lb > RD_CAP) enter_dense(W, wg, k);  // W outgrows its buffer
+      if (dense) {
+        k += dense_flip(D, pool + at_o + 1, true, lb, row_base);
+        ++n_merges;
+        published = false;
+        if (k == 0) {
+          leave_dense();
+          break;
+        }
+        D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+        continue;
+      }
       if (!wg && lb <= 31 && k + lb <= RD_CAP) {
         const int m = warp_xor_small<false>(W, k, lane < lb ? bv : INT_MAX, lb, (sW0 + (cur ^ 1) * RD_CAP));
         __syncwarp();
@@ -538,6 +661,7 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
         published = false;
       }
     }
+    leave_dense();  // every exit leaves the slot clean for the next column
     }
   }
   if (lane == 0) {
@@ -589,8 +713,28 @@ inline int grid_for(i64 n, int nt = 256) {
 
 using namespace ph;
 
+// Grid of k_reduce on the current device: persistent blocks, one per resident slot.
+int reduce_blocks(i64 K) {
+  int dev = 0, sms = 148, occ = 1;
+  ph::allow_dynamic_smem((const void*)k_reduce);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_reduce, RD_NT, RD_SMEM);
+  return (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
+}
+
+// dense working-column slots: one bitmap of R bits per warp of the grid, when
+// they fit in 1 GiB (else long columns stay sorted lists in the pool)
+i64 dense_words(i64 K, i64 R) {
+  const i64 words = (R + 31) / 32 + 1;
+  const i64 warps = (i64)reduce_blocks(K) * RD_WARPS;
+  return words * warps * 4 <= (i64(1) << 30) ? words : 0;
+}
+
 extern "C" size_t ph_reduce_workspace_bytes(int64_t K, int64_t R) {
-  return Carve::need((size_t)R * 8) + Carve::need((size_t)K * 8) + Carve::need(sizeof(RedCtl));
+  const i64 dw = K > 0 ? dense_words(K, R) : 0;
+  return Carve::need((size_t)R * 8) + Carve::need((size_t)K * 8) + Carve::need(sizeof(RedCtl)) +
+         (dw ? Carve::need((size_t)dw * 4 * reduce_blocks(K) * RD_WARPS) : 0);
 }
 
 extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,
@@ -617,24 +761,19 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   ph::count_launch();
   k_classify<<<grid_for(K), 256, 0, s>>>(cof_off, cof_data, K, col_base, row_base, skip, row_cmf, col_state,
                                          col_piv, owner, rec, pool, pool_cap, ctl, d_status);
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaFuncSetAttribute(k_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RD_SMEM) != cudaSuccess) {
+  if (ph::allow_dynamic_smem((const void*)k_reduce) != cudaSuccess) {
     PH_CHECK_LAUNCH();
     return PH_ERR_CUDA;
   }
-  int occ = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_reduce, RD_NT, RD_SMEM);
-  // residual count is known only on the device; K bounds it. Blocks are
-  // persistent (a shared work counter), so only resident blocks are launched.
-  const int blocks =
-      (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
+  const int blocks = reduce_blocks(K);
+  const i64 dw = dense_words(K, R);
+  u32* dense = dw ? c.take<u32>(dw * (i64)blocks * RD_WARPS) : nullptr;
+  if (dw && !dense) return PH_ERR_ARG;
   // pool chunk per warp: small enough that the chunks of all warps fit a quarter of the pool
   const int chunk = (int)std::max<i64>(64, std::min<i64>(2048, pool_cap / (4 * (i64)blocks * RD_WARPS)));
   ph::count_launch();
   k_reduce<<<blocks, RD_NT, RD_SMEM, s>>>(row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
-                                          1 << 24);
+                                          1 << 24, dense, dw);
   ph::count_launch();
   k_finish_cols<<<grid_for(K), 256, 0, s>>>(K, col_state, col_piv, ctl, d_info);
   if (R > 0) {

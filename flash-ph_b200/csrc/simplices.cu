@@ -93,6 +93,54 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
   }
 }
 
+// Exact number of triangles of the graph (each counted once, at its smallest
+// vertex x and middle vertex y: pairs x < y < z, all three edges present).
+// One CTA per vertex a (persistent over vertices): N(a) goes into a shared
+// bitmap, each warp takes a neighbour b > a and tests its neighbours w > b
+// against the bitmap. No ranks are needed, since every triangle has exactly
+// one largest edge; the result equals the sum of the per-edge triangle counts.
+__global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ aptr, const i32* __restrict__ aidx,
+                                                    i64 n, int* __restrict__ next,
+                                                    unsigned long long* __restrict__ total) {
+  extern __shared__ u32 nbits[];
+  __shared__ int cur;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const i64 words = (n + 31) >> 5;
+  for (i64 w = threadIdx.x; w < words; w += SX_NT) nbits[w] = 0u;
+  unsigned long long cnt = 0;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) cur = atomicAdd(next, 1);
+    __syncthreads();
+    const i64 a = cur;
+    if (a >= n) break;
+    const int s = aptr[a], e = aptr[a + 1];
+    if (e - s < 2) continue;
+    for (int p = s + threadIdx.x; p < e; p += SX_NT) {
+      const i32 v = aidx[p];
+      atomicOr(&nbits[v >> 5], 1u << (v & 31));
+    }
+    __syncthreads();
+    // neighbours b > a of a (rows sorted by neighbour index)
+    const int first = lower_bound_i32(aidx, s, e, (i32)a + 1);
+    for (int p = first + warp; p < e; p += SX_NT / 32) {
+      const i32 b = aidx[p];
+      const int sb = aptr[b], eb = aptr[b + 1];
+      for (int q = lower_bound_i32(aidx, sb, eb, b + 1) + lane; q < eb; q += 32) {
+        const i32 w = aidx[q];
+        cnt += (nbits[w >> 5] >> (w & 31)) & 1u;
+      }
+    }
+    __syncthreads();
+    for (int p = s + threadIdx.x; p < e; p += SX_NT) {
+      const i32 v = aidx[p];
+      nbits[v >> 5] = 0u;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
+  if (lane == 0 && cnt) atomicAdd(total, cnt);
+}
+
 // Tetrahedra with largest edge m: pairs (i < k) of m's triangles whose third
 // vertices p = W[i], q = W[k] are joined by an edge ranked below m.
 template <bool EMIT>
@@ -245,6 +293,38 @@ extern "C" int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, 
   }
   PH_TRY(scan_exclusive_i32_i64(tc, tri_off, E, sws, scan_workspace_bytes(E), s));
   PH_TRY(scan_exclusive_i32_i64(cc, cof_off, E, sws, scan_workspace_bytes(E), s));
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int64_t ph_triangles_total_max_vertices(void) { return (int64_t)(200 * 1024) * 8; }
+
+extern "C" int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx, int64_t n,
+                                  unsigned long long* d_total, int* d_next, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n < 0 || !d_total || !d_next) return PH_ERR_ARG;
+  if (n > ph_triangles_total_max_vertices()) {
+    record_message("ph_triangles_total: n exceeds the shared-memory bitmap (1638400 vertices)");
+    return PH_ERR_ARG;
+  }
+  cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s);
+  cudaMemsetAsync(d_next, 0, sizeof(int), s);
+  if (n < 3) {
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  const size_t smem = (size_t)((n + 31) / 32) * 4;
+  if (smem > 48 * 1024 && ph::allow_dynamic_smem((const void*)k_tri_total) != cudaSuccess) {
+    PH_CHECK_LAUNCH();
+    return PH_ERR_CUDA;
+  }
+  int dev = 0, sms = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tri_total, SX_NT, smem);
+  const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
+  ph::count_launch();
+  k_tri_total<<<grid, SX_NT, smem, s>>>(adj_ptr, adj_idx, n, d_next, d_total);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -140,7 +140,7 @@ extern "C" int ph_knn_kth(const float* pts, int64_t n, int32_t d, int32_t k, flo
   if (n == 0) return PH_OK;
   const size_t smem = knn_smem(d);
   if (smem > 200 * 1024) return PH_ERR_ARG;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_knn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_knn);
   ph::count_launch();
   k_knn<<<(unsigned)((n + KN_NT - 1) / KN_NT), KN_NT, smem, (cudaStream_t)stream>>>(pts, n, d, k, out);
   PH_CHECK_LAUNCH();
@@ -185,8 +185,7 @@ extern "C" int ph_enclosing_radius(const float* pts, int64_t n, int32_t d, float
   if (!bits) return PH_ERR_ARG;
   const size_t smem = knn_smem(d);
   if (smem > 200 * 1024) return PH_ERR_ARG;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_enclosing, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_enclosing);
   cudaMemsetAsync(bits, 0x7f, sizeof(unsigned int), s);
   ph::count_launch();
   k_enclosing<<<(unsigned)((n + KN_NT - 1) / KN_NT), KN_NT, smem, s>>>(pts, n, d, bits);

@@ -25,7 +25,7 @@ from torch import Tensor
 
 from . import _lib as L
 from .boruvka import boruvka_mask
-from .cohomology import Reduction, cof_max_face, cofacet_csr, reduce as _reduce
+from .cohomology import Reduction, cof_max_face, cofacet_csr, grow_pool, pool_capacity, reduce as _reduce
 from .rips import edge_filtration_values, threshold_sq, vertex_csr
 
 PH_ERR_POOL = 5
@@ -264,8 +264,7 @@ def _run_chunk(pts_list, thrs, dims, device, max_triangles, max_tetrahedra):
 def _reduce_retry(off, data, K, col_base, R, row_base, skip, cmf, checks):
     """Reduction whose status is read with the final synchronisation; a pool
     overflow (rare) is detected here by a synchronous check and retried."""
-    nnz = int(data.numel())
-    pool_cap = max(16 * nnz + 2 * K, 1 << 22)
+    pool_cap = pool_capacity(int(data.numel()), K)
     for _ in range(4):
         red = _reduce(off, data, K, col_base, R, row_base, skip, cmf, pool_cap)
         st = int(red.status.item())
@@ -273,7 +272,7 @@ def _reduce_retry(off, data, K, col_base, R, row_base, skip, cmf, checks):
             return red
         if st != PH_ERR_POOL:
             raise L.PHError("ph_reduce", st)
-        pool_cap *= 4
+        pool_cap = grow_pool(pool_cap)
     raise L.PHError("ph_reduce", PH_ERR_POOL, "pool still too small after retries")
 
 

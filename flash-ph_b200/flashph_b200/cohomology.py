@@ -130,6 +130,25 @@ def persistence_rows(red: Reduction, K: int, row_base: int, filt: Tensor, col_m,
     return rows, nrows
 
 
+# record offsets in the reducer's owner words have 33 bits
+_POOL_MAX = (1 << 33) - 1
+
+
+def pool_capacity(nnz: int, K: int) -> int:
+    """Initial reduction pool (int32 entries): the initial records (at most
+    2 nnz), per-warp chunks and the reduced columns; generous for small
+    problems, where a retry would cost more than the memory, and bounded by
+    the record-offset range."""
+    mult = 8 if nnz < (1 << 24) else 3
+    return min(mult * nnz + 2 * K + (1 << 23), _POOL_MAX)
+
+
+def grow_pool(cap: int) -> int:
+    if cap >= _POOL_MAX:
+        raise L.PHError("ph_reduce", PH_ERR_POOL, "pool at its maximum size")
+    return min(cap * 4, _POOL_MAX)
+
+
 def _reduce_to_rows(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, filt, col_m, row_m,
                     checks=()):
     """Reduction + rows with one host synchronisation; grows the pool on demand.
@@ -137,8 +156,7 @@ def _reduce_to_rows(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, filt
     ``checks``: (entry point name, device status tensor) pairs of earlier
     stages, read back in the same copy and raised if non-zero.
     """
-    nnz = int(cof_data.numel())
-    pool_cap = max(16 * nnz + 2 * K, 1 << 22)
+    pool_cap = pool_capacity(int(cof_data.numel()), K)
     for _ in range(_MAX_POOL_RETRIES):
         red = reduce(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, pool_cap)
         rows, nrows = persistence_rows(red, K, row_base, filt, col_m, row_m)
@@ -152,7 +170,7 @@ def _reduce_to_rows(cof_off, cof_data, K, col_base, R, row_base, skip, cmf, filt
             return rows[: int(host[1])], red, host[2:6]
         if st != PH_ERR_POOL:
             raise L.PHError("ph_reduce", st)
-        pool_cap *= 4
+        pool_cap = grow_pool(pool_cap)
     raise L.PHError("ph_reduce", PH_ERR_POOL, "pool still too small after retries")
 
 

@@ -1,14 +1,16 @@
 """Serving form: a continuous-batching request loop on one GPU.
 
 ``PersistenceServer.submit(points, max_edge_length, max_dim)`` returns a
-future. Worker slots (one CUDA stream each) take every queued request that
-fits the admission limits, run them as one batch through the batching
-pipeline (``batch.rips_persistence_batch``) and resolve the futures; while
-one slot's batch is on the device, the next slot admits the requests that
-arrived in the meantime, so batches overlap on the GPU. Admission is by
-memory, estimated from the request sizes (points, candidate pairs); the
-pipeline's own counting pass then enforces the reference's per-call
-triangle and tetrahedron caps per request.
+future. Worker slots (one CUDA stream each) take work from the queue: a
+request of at least ``solo_min_points`` points runs alone through the native
+pipeline (``ph_rips_persistence``, one library call that waits on the host
+four times at most); the small requests at the head of the queue that fit
+the admission limits run together as one batch through the batching
+pipeline (``batch.rips_persistence_batch``). While one slot waits on the
+host, another slot's work runs on the GPU. Admission is by memory, estimated
+from the request sizes (points, candidate pairs); the pipelines' own
+counting passes enforce the reference's per-call triangle and tetrahedron
+caps per request.
 
 Every result equals what ``rips_persistence`` returns for that request
 alone, bit for bit: requests never interact inside a batch.
@@ -24,6 +26,7 @@ import numpy as np
 import torch
 
 from .batch import rips_persistence_batch
+from .persistence import rips_persistence
 
 
 class _Request:
@@ -48,11 +51,13 @@ class PersistenceServer:
     max_batch_points : admission limit on the points of one batch.
     max_batch_pairs : admission limit on candidate point pairs of one batch.
     max_batch_requests : admission limit on requests per batch.
+    solo_min_points : requests this large run alone (native pipeline).
     """
 
-    def __init__(self, device=None, slots: int = 2, max_batch_points: int = 1 << 17,
+    def __init__(self, device=None, slots: int = 3, max_batch_points: int = 1 << 17,
                  max_batch_pairs: int = 1 << 32, max_batch_requests: int = 1024,
-                 max_triangles: int = 10_000_000, max_tetrahedra: int = 10_000_000):
+                 max_triangles: int = 10_000_000, max_tetrahedra: int = 10_000_000,
+                 solo_min_points: int = 0):
         if not torch.cuda.is_available():
             raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -61,6 +66,7 @@ class PersistenceServer:
         self.max_batch_requests = max_batch_requests
         self.max_triangles = max_triangles
         self.max_tetrahedra = max_tetrahedra
+        self.solo_min_points = solo_min_points
         self._queue: collections.deque[_Request] = collections.deque()
         self._cv = threading.Condition()
         self._closed = False
@@ -94,10 +100,14 @@ class PersistenceServer:
         self.close()
 
     def _admit(self) -> list[_Request]:
+        if self._queue[0].n >= self.solo_min_points:
+            return [self._queue.popleft()]
         batch, pts, pairs = [], 0, 0
         while self._queue and len(batch) < self.max_batch_requests:
             r = self._queue[0]
             n = r.n
+            if n >= self.solo_min_points:
+                break
             if batch and (pts + n > self.max_batch_points or pairs + n * n // 2 > self.max_batch_pairs):
                 break
             batch.append(self._queue.popleft())
@@ -117,9 +127,16 @@ class PersistenceServer:
                 batch = self._admit()
             try:
                 with torch.cuda.stream(stream):
-                    res = rips_persistence_batch([r.points for r in batch], [r.t for r in batch],
-                                                 [r.max_dim for r in batch], self.max_triangles,
-                                                 self.max_tetrahedra)
+                    if len(batch) == 1 and batch[0].n >= self.solo_min_points:
+                        r = batch[0]
+                        try:
+                            res = [rips_persistence(r.points, r.t, max_dim=r.max_dim)]
+                        except ValueError as ex:  # the reference's per-call errors
+                            res = [ex]
+                    else:
+                        res = rips_persistence_batch([r.points for r in batch], [r.t for r in batch],
+                                                     [r.max_dim for r in batch], self.max_triangles,
+                                                     self.max_tetrahedra)
                 stream.synchronize()
                 self.batches += 1
             except Exception as ex:  # a failure of the whole batch goes to each request

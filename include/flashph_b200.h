@@ -178,6 +178,17 @@ int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
                        int64_t* tri_off, int64_t* cof_off, void* workspace,
                        size_t workspace_bytes, void* stream);
 
+/* Exact number of triangles of the graph (the sum of ph_triangles_count's
+ * per-edge counts), without ranks: each triangle x < y < z is found once from
+ * a shared-memory bitmap of N(x). Work ~ sum over vertices of deg^2 / 6
+ * bitmap tests, far below the per-edge count's searches on dense graphs; used
+ * to check the reference's max_triangles limit (triangle_kernel.py:377-381)
+ * before the per-edge pass. n <= ph_triangles_total_max_vertices(); d_next:
+ * one int of device scratch. */
+int64_t ph_triangles_total_max_vertices(void);
+int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx, int64_t n,
+                       unsigned long long* d_total, int* d_next, void* stream);
+
 /* Writes, for every triangle in global order, its largest edge tri_m, third
  * vertex tri_w and the ranks of its two other edges (a,w) and (b,w). */
 int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E,

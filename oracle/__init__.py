@@ -22,7 +22,7 @@ ARRAYS = ("edge_i", "edge_j", "edge_dsq", "mst_idx", "h0", "tri_max_rank_sorted"
           "ap_births", "ap_deaths", "res_births", "res_deaths", "ess_births",
           "h1_all_pivots", "h1", "h2", "h2_births", "h2_deaths", "h2_ess")
 SCALARS = ("E", "n_components", "T", "Q", "cofacet_nnz", "n_apparent", "residual", "xor_ops",
-           "xor_max", "xor_elems", "crit_path")
+           "xor_max", "xor_elems", "crit_path", "col_max")
 
 
 def build(force: bool = False) -> str:

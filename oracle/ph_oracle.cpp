@@ -38,6 +38,7 @@ struct Result {
   i64 T = 0, cofacet_nnz = 0, n_apparent = 0, residual = 0;
   i64 xor_ops = 0, xor_max = 0, xor_elems = 0;  // reduction work statistics
   i64 crit_path = 0;  // H1: longest chain of dependent additions (each waits for the column it adds)
+  i64 col_max = 0;    // H1: largest working column (entries) met during the reduction
   std::vector<i32> tri_max_rank_sorted;
   std::vector<i32> ap_births, ap_deaths, res_births, res_deaths, ess_births;
   std::vector<i32> h1_all_pivots;
@@ -430,6 +431,7 @@ void h1_native(Result& R, i64 n, const CSR& g, const Triangles& tr, const std::v
       step = std::max(step, dt == done_at.end() ? (i64)0 : dt->second) + 1;
       R.xor_elems += (i64)(cur.size() + it->second.size());
       xor_into(cur, it->second, tmp);
+      R.col_max = std::max<i64>(R.col_max, (i64)cur.size());
       ++ops;
     }
     R.crit_path = std::max(R.crit_path, step);
@@ -698,6 +700,7 @@ int64_t oracle_scalar(void* h, const char* name) {
   if (s == "xor_max") return R->xor_max;
   if (s == "xor_elems") return R->xor_elems;
   if (s == "crit_path") return R->crit_path;
+  if (s == "col_max") return R->col_max;
   return -1;
 }
 

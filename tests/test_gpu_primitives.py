@@ -64,3 +64,28 @@ def test_launch_counter_advances():
     sort_edges(torch.from_numpy(ei).cuda(), torch.from_numpy(ej).cuda(), torch.from_numpy(ed).cuda(), 100)
     torch.cuda.synchronize()
     assert _lib.launch_count() > before
+
+
+@pytest.mark.parametrize("n,d,t", [(500, 3, 0.3), (2000, 4, 0.9), (1500, 10, 3.0), (800, 2, 5.0), (3, 2, 9.0)])
+def test_triangle_total_equals_per_edge_counts(n, d, t):
+    """ph_triangles_total (rank-free, bitmap) equals the sum of the per-edge
+    triangle counts on sparse, dense and complete graphs."""
+    from flashph_b200 import _lib as L
+    from flashph_b200.cohomology import count_triangles
+    from flashph_b200.rips import rips_filtration
+    x = torch.from_numpy(np.random.default_rng(n + d).standard_normal((n, d)).astype(np.float32)).cuda()
+    f = rips_filtration(x, t)
+    E = f.edge_i.shape[0]
+    want = int(count_triangles(f)[E].item())
+    tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+    nxt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    L.call("ph_triangles_total", f.vert_adj_ptr.data_ptr(), f.vert_adj_idx.data_ptr(), n, tot.data_ptr(),
+           nxt.data_ptr(), L.stream_handle(x.device))
+    assert int(tot.item()) == want
+
+
+def test_dense_call_over_the_triangle_limit_reports_the_exact_count():
+    from flashph_b200 import rips_persistence
+    pts = np.random.default_rng(5).standard_normal((3000, 3)).astype(np.float32)
+    with pytest.raises(ValueError, match="Triangle count 4495501000 exceeds max_triangles=10000000"):
+        rips_persistence(torch.from_numpy(pts).cuda(), 1e3, max_dim=1)  # complete graph: C(3000, 3)

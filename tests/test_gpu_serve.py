@@ -61,3 +61,35 @@ def test_served_errors_are_per_request():
             f2.result(timeout=120)
         with pytest.raises(ValueError, match="H2 requires n < 65536"):
             f3.result(timeout=120)
+
+
+def test_solo_and_batched_slots_run_concurrently():
+    """Three slots on their own streams, large requests alone through the
+    native pipeline and small ones batched, clouds of three dimensions (both
+    edge kernels) in flight together: every result equals the alone result."""
+    from flashph_b200 import rips_persistence
+    from flashph_b200.serve import PersistenceServer
+    rng = np.random.default_rng(31)
+    reqs = []
+    for i in range(40):
+        n = int(np.exp(rng.uniform(np.log(50), np.log(9000))))
+        d = int(rng.choice([4, 10, 50]))
+        t = {4: 0.35, 10: 1.3, 50: 6.3}[d]
+        reqs.append((rng.standard_normal((n, d)).astype(np.float32), t, 2 if n < 3000 and i % 5 == 0 else 1))
+    with PersistenceServer(slots=3, solo_min_points=2000, max_batch_points=6000) as srv:
+        futs = [srv.submit(p, t, md) for p, t, md in reqs]
+        served = []
+        for f in futs:
+            try:
+                served.append(f.result(timeout=300))
+            except ValueError as ex:
+                served.append(ex)
+    for (p, t, md), got in zip(reqs, served):
+        try:
+            alone = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=md)
+        except ValueError as ex:
+            assert isinstance(got, ValueError) and str(got) == str(ex)
+            continue
+        assert not isinstance(got, Exception), got
+        for a, b in zip(got, alone):
+            assert a.shape == b.shape and np.array_equal(_bits(a), _bits(b))
