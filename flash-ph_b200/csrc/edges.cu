@@ -199,25 +199,27 @@ __global__ void k_gather_edges(const u32* __restrict__ perm, const i32* __restri
 }
 
 // ---- vertex CSR ---------------------------------------------------------------
-__global__ void k_half_keys(const i32* __restrict__ ei, const i32* __restrict__ ej, i64 E,
+// half-edge keys (vertex << sh) | neighbour, sh = the bits of a vertex index
+__global__ void k_half_keys(const i32* __restrict__ ei, const i32* __restrict__ ej, i64 E, int sh,
                             u64* __restrict__ keys, u32* __restrict__ vals) {
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     const u64 i = (u64)(u32)ei[e], j = (u64)(u32)ej[e];
-    keys[2 * e] = (i << 32) | j;
+    keys[2 * e] = (i << sh) | j;
     vals[2 * e] = (u32)e;
-    keys[2 * e + 1] = (j << 32) | i;
+    keys[2 * e + 1] = (j << sh) | i;
     vals[2 * e + 1] = (u32)e;
   }
 }
 
-__global__ void k_csr_fill(const u64* __restrict__ keys, const u32* __restrict__ vals, i64 H, i64 n,
+__global__ void k_csr_fill(const u64* __restrict__ keys, const u32* __restrict__ vals, i64 H, i64 n, int sh,
                            i32* __restrict__ ptr, i32* __restrict__ idx, i32* __restrict__ rank) {
+  const u64 low = (1ull << sh) - 1;
   for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < H; p += (i64)gridDim.x * blockDim.x) {
     const u64 k = keys[p];
-    const i64 s = (i64)(k >> 32);
-    idx[p] = (i32)(k & 0xffffffffull);
+    const i64 s = (i64)(k >> sh);
+    idx[p] = (i32)(k & low);
     rank[p] = (i32)vals[p];
-    const i64 prev = p ? (i64)(keys[p - 1] >> 32) : -1;
+    const i64 prev = p ? (i64)(keys[p - 1] >> sh) : -1;
     for (i64 v = prev + 1; v <= s; ++v) ptr[v] = (i32)p;
     if (p == H - 1)
       for (i64 v = s + 1; v <= n; ++v) ptr[v] = (i32)H;
@@ -327,11 +329,15 @@ extern "C" int ph_vertex_csr(const int32_t* edge_i, const int32_t* edge_j, int64
   u32* vals = c.take<u32>(2 * E);
   void* rws = c.take<char>((i64)radix_sort_workspace_bytes(2 * E));
   if (!keys || !vals || !rws) return PH_ERR_ARG;
+  // sort only the key bits a vertex pair needs: 2 x bits(n - 1), in whole bytes
+  int sh = 1;
+  while (sh < 32 && (int64_t(1) << sh) < n) ++sh;
+  const int end_bit = std::min(64, ((2 * sh + 7) / 8) * 8);
   ph::count_launch();
-  k_half_keys<<<grid_for(E), 256, 0, s>>>(edge_i, edge_j, E, keys, vals);
-  PH_TRY(radix_sort_pairs(keys, vals, 2 * E, 0, 64, rws, radix_sort_workspace_bytes(2 * E), s));
+  k_half_keys<<<grid_for(E), 256, 0, s>>>(edge_i, edge_j, E, sh, keys, vals);
+  PH_TRY(radix_sort_pairs(keys, vals, 2 * E, 0, end_bit, rws, radix_sort_workspace_bytes(2 * E), s));
   ph::count_launch();
-  k_csr_fill<<<grid_for(2 * E), 256, 0, s>>>(keys, vals, 2 * E, n, adj_ptr, adj_idx, adj_rank);
+  k_csr_fill<<<grid_for(2 * E), 256, 0, s>>>(keys, vals, 2 * E, n, sh, adj_ptr, adj_idx, adj_rank);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -406,7 +406,11 @@ extern "C" int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const
   if (!keys || !vals || !rws) return PH_ERR_ARG;
   ph::count_launch();
   k_cof_entries<<<grid_for(H), 256, 0, s>>>(faces_aos, f0, f1, f2, k, S, row_base, keys, vals);
-  PH_TRY(radix_sort_pairs(keys, vals, H, 0, 32, rws, radix_sort_workspace_bytes(H), s));
+  // face indices are below n_faces: sort only the bytes they use (stable, so
+  // the simplices of a face stay in ascending order)
+  int fb = 1;
+  while (fb < 32 && (int64_t(1) << fb) < n_faces) ++fb;
+  PH_TRY(radix_sort_pairs(keys, vals, H, 0, std::min(32, ((fb + 7) / 8) * 8), rws, radix_sort_workspace_bytes(H), s));
   ph::count_launch();
   k_cof_fill<<<grid_for(H), 256, 0, s>>>(keys, vals, H, n_faces, cof_off, cof_data);
   PH_CHECK_LAUNCH();

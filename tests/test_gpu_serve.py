@@ -27,7 +27,7 @@ def test_served_results_equal_alone_results():
         t = {4: 0.9, 10: 2.4, 50: 7.2}[d]
         md = 2 if (rng.random() < 0.2 and n < 600) else 1
         reqs.append((rng.standard_normal((n, d)).astype(np.float32), t, md))
-    with PersistenceServer(slots=2, max_batch_points=4000) as srv:
+    with PersistenceServer(slots=2, max_batch_points=4000, solo_min_points=1 << 30) as srv:
         futs = [None] * len(reqs)
 
         def producer(lo, hi):
