@@ -166,9 +166,16 @@ __global__ void __launch_bounds__(RS_NT) k_os_hist(const u64* __restrict__ keys,
   __shared__ u32 h[8][256];
   for (int i = threadIdx.x; i < 8 * 256; i += RS_NT) h[i >> 8][i & 255] = 0;
   __syncthreads();
-  for (i64 i = (i64)blockIdx.x * RS_NT + threadIdx.x; i < n; i += (i64)gridDim.x * RS_NT) {
-    const u64 k = keys[i];
-    for (int p = p0; p < p1; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255u], 1u);
+  // four keys per thread and step, loaded before they are counted
+  const i64 step = (i64)gridDim.x * RS_NT * 4;
+  for (i64 b = (i64)blockIdx.x * RS_NT * 4 + threadIdx.x; b < n; b += step) {
+    u64 k4[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) k4[q] = b + q * RS_NT < n ? __ldg(keys + b + q * RS_NT) : 0ull;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (b + q * RS_NT < n)
+        for (int p = p0; p < p1; ++p) atomicAdd(&h[p][(k4[q] >> (8 * p)) & 255u], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 8 * 256; i += RS_NT) {
@@ -179,24 +186,39 @@ __global__ void __launch_bounds__(RS_NT) k_os_hist(const u64* __restrict__ keys,
 
 // Number of active passes before `pass` and whether `pass` itself is active.
 __device__ __forceinline__ void pass_plan(const SortCtl* ctl, i64 n, int p0, int pass, int* before,
-                                          bool* active) {
+                                          bool* active, u32* count) {
+  // the histogram words first (independent loads), then one barrier per pass
+  u32 g[8];
+#pragma unroll
+  for (int p = 0; p < 8; ++p) g[p] = (p >= p0 && p <= pass) ? ctl->ghist[p][threadIdx.x] : 0u;
   int cnt = 0;
   bool act = false;
-  for (int p = p0; p <= pass; ++p) {
-    const int full = __syncthreads_or(ctl->ghist[p][threadIdx.x] == (u32)n);
+#pragma unroll
+  for (int p = 0; p < 8; ++p) {
+    if (p < p0 || p > pass) continue;
+    const int full = __syncthreads_or(g[p] == (u32)n);
     if (p < pass) cnt += !full;
     else act = !full;
   }
   *before = cnt;
   *active = act;
+  u32 c = 0;
+#pragma unroll
+  for (int p = 0; p < 8; ++p)
+    if (p == pass) c = g[p];
+  *count = c;
 }
 
 __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u32* vB, i64 n, int p0,
                                                   int pass, SortCtl* ctl, unsigned long long* lb,
                                                   i64 ntiles) {
+  __shared__ u32 tile_sh;
+  // the first ticket is taken before the plan so that its latency overlaps it
+  if (threadIdx.x == 0) tile_sh = atomicAdd(&ctl->ticket[pass], 1u);
   int before;
   bool active;
-  pass_plan(ctl, n, p0, pass, &before, &active);
+  u32 v;
+  pass_plan(ctl, n, p0, pass, &before, &active, &v);
   if (!active) return;
   const bool srcB = before & 1;
   const u64* ks = srcB ? kB : kA;
@@ -209,10 +231,8 @@ __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u3
   __shared__ u32 gstart[256];
   __shared__ u32 tbase[256];
   __shared__ u32 wsum[RS_WARPS];
-  __shared__ i64 tile_sh;
   // exclusive scan of the global digit counts of this pass
   {
-    const u32 v = ctl->ghist[pass][threadIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     u32 x = v;
 #pragma unroll
@@ -228,22 +248,33 @@ __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u3
   }
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const u32 lt = lanemask_lt();
+  __syncthreads();
+  i64 tile = tile_sh;
   for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) tile_sh = atomicAdd(&ctl->ticket[pass], 1u);
     for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_NT) cnt[i >> 8][i & 255] = 0;
-    __syncthreads();
-    const i64 tile = tile_sh;
+    __syncthreads();  // every thread has read tile_sh; counters cleared
     if (tile >= ntiles) break;
+    // the next ticket is in flight while this tile is sorted; a held ticket
+    // never blocks progress, since the lowest unfinished tile is always held
+    // by a running block whose earlier tiles are done
+    u32 next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(&ctl->ticket[pass], 1u);
     const i64 wbase = tile * RS_TILE + (i64)w * RS_PER_WARP;
     u64 key[RS_ROUNDS];
     u32 val[RS_ROUNDS], dig[RS_ROUNDS], pos[RS_ROUNDS];
+    // all loads first (independent, in flight together), then the counting rounds
+#pragma unroll
+    for (int r = 0; r < RS_ROUNDS; ++r) {
+      const i64 i = wbase + r * 32 + lane;
+      key[r] = i < n ? __ldg(ks + i) : 0ull;
+      val[r] = i < n ? __ldg(vs + i) : 0u;
+    }
 #pragma unroll
     for (int r = 0; r < RS_ROUNDS; ++r) {
       const i64 i = wbase + r * 32 + lane;
       const bool ok = i < n;
-      const u64 k = ok ? ks[i] : 0ull;
-      const u32 v = ok ? vs[i] : 0u;
+      const u64 k = key[r];
+      const u32 v = val[r];
       const u32 d = ok ? (u32)((k >> shift) & 255u) : 256u;
       const u32 peers = __match_any_sync(FULL, d);
       const u32 rank = __popc(peers & lt);
@@ -272,23 +303,40 @@ __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u3
       tbase[dgt] = gstart[dgt];
     } else {
       *slot = epoch | LB_AGG | total;
+      // look back over the predecessors, eight slots per step (independent
+      // loads), summing aggregates until an inclusive prefix is found
       u32 excl = 0;
       i64 t = tile - 1;
       int spins = 0;
+      constexpr int LB_BATCH = 8;
       while (t >= 0) {
-        const volatile unsigned long long* vp = lb + t * 256 + dgt;
-        const unsigned long long cur = *vp;
-        if ((cur & ~((1ull << 40) - 1)) != epoch || ((cur >> 32) & 0xffull) == 0) {
+        unsigned long long cur[LB_BATCH];
+#pragma unroll
+        for (int q = 0; q < LB_BATCH; ++q)
+          cur[q] = (t - q >= 0) ? *(const volatile unsigned long long*)(lb + (t - q) * 256 + dgt) : 0ull;
+        bool done = false, wait = false;
+        int used = 0;
+#pragma unroll
+        for (int q = 0; q < LB_BATCH; ++q) {
+          if (done || wait || t - q < 0) continue;
+          const unsigned long long c = cur[q];
+          if ((c & ~((1ull << 40) - 1)) != epoch || ((c >> 32) & 0xffull) == 0) {
+            wait = true;  // not published yet: retry from this slot
+            continue;
+          }
+          excl += (u32)(c & 0xffffffffull);
+          ++used;
+          if (c & LB_PRE) done = true;
+        }
+        if (done) break;
+        t -= used;
+        if (wait) {
           if (++spins > LB_SPIN_LIMIT) {
             atomicExch(&ctl->error, 1);
             break;
           }
           __nanosleep(32);
-          continue;
         }
-        excl += (u32)(cur & 0xffffffffull);
-        if (cur & LB_PRE) break;
-        --t;
       }
       *slot = epoch | LB_PRE | (excl + total);
       tbase[dgt] = gstart[dgt] + excl;
@@ -303,13 +351,21 @@ __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u3
         vd[o] = val[r];
       }
     }
+    if (threadIdx.x == 0) tile_sh = next;
+    __syncthreads();
+    tile = tile_sh;
   }
 }
 
 __global__ void k_os_finish(u64* __restrict__ kA, u32* __restrict__ vA, const u64* __restrict__ kB,
                             const u32* __restrict__ vB, i64 n, int p0, int p1, const SortCtl* ctl) {
+  u32 g[8];
+#pragma unroll
+  for (int p = 0; p < 8; ++p) g[p] = (p >= p0 && p < p1) ? ctl->ghist[p][threadIdx.x] : 0u;
   int act = 0;
-  for (int p = p0; p < p1; ++p) act += !__syncthreads_or(ctl->ghist[p][threadIdx.x] == (u32)n);
+#pragma unroll
+  for (int p = 0; p < 8; ++p)
+    if (p >= p0 && p < p1) act += !__syncthreads_or(g[p] == (u32)n);
   if (!(act & 1)) return;
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
     kA[i] = kB[i];
@@ -357,7 +413,7 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
   const size_t clear = (size_t)((char*)(lb + ntiles * 256) - (char*)ctl);
   cudaMemsetAsync(ctl, 0, clear, s);
   const int p0 = begin_bit / 8, p1 = end_bit / 8;
-  const int gh = (int)std::max<i64>(1, std::min<i64>((n + RS_NT * 16 - 1) / (RS_NT * 16), 296));
+  const int gh = (int)std::max<i64>(1, std::min<i64>((n + RS_NT * 4 - 1) / (RS_NT * 4), 592));
   ph::count_launch();
   k_os_hist<<<gh, RS_NT, 0, s>>>(keys, n, p0, p1, ctl);
   const int gp = (int)std::min<i64>(ntiles, 148 * 4);

@@ -151,9 +151,13 @@ __device__ __forceinline__ i32 ld(const i32* p) {
 }
 
 // out = L xor S for L (<= 32 MR entries) and S (ns <= 32, one per lane in sv)
-// with everything in registers: L is loaded 32 entries per round, S_j is
-// ranked in L by ballots, and each L entry counts the insertion points below
-// it with broadcast shuffles (independent, so their latencies overlap).
+// with L in registers. An element's output position is its rank in its own
+// list plus its rank in the other list, less twice the common values below
+// it; common values are dropped. Ranks of L entries in S come from a
+// branch-free lower bound over the lanes holding S (five shuffles plus one
+// for the 32nd lane), ranks of S entries in L the same way over L's lanes
+// (MR = 1) or a binary search of L (MR > 1). The searches of the MR chunks are
+// independent, so their latencies overlap.
 template <bool G, int MR>
 __device__ int warp_xor_tiny(const i32* L, int nl, i32 sv, int ns, i32* out) {
   const int lane = threadIdx.x & 31;
@@ -161,48 +165,60 @@ __device__ int warp_xor_tiny(const i32* L, int nl, i32 sv, int ns, i32* out) {
   i32 lr[MR];
 #pragma unroll
   for (int m = 0; m < MR; ++m) lr[m] = (lane + 32 * m < nl) ? ld<G>(L + lane + 32 * m) : INT_MAX;
-  int c[MR], dc[MR];
-  bool del[MR];
+  const i32 s31 = __shfl_sync(FULL, sv, 31);
+  int rs[MR];
+#pragma unroll
+  for (int m = 0; m < MR; ++m) rs[m] = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+#pragma unroll
+    for (int m = 0; m < MR; ++m) {
+      const i32 y = __shfl_sync(FULL, sv, rs[m] + step - 1);
+      if (y < lr[m]) rs[m] += step;
+    }
+  }
+  bool eqL[MR];
+  u32 dmL[MR];
 #pragma unroll
   for (int m = 0; m < MR; ++m) {
-    c[m] = 0;
-    dc[m] = 0;
-    del[m] = false;
+    if (rs[m] == 31 && s31 < lr[m]) rs[m] = 32;
+    const i32 y = __shfl_sync(FULL, sv, rs[m] & 31);
+    eqL[m] = lane + 32 * m < nl && rs[m] < ns && y == lr[m];
+    dmL[m] = __ballot_sync(FULL, eqL[m]);
   }
-  int mypos = nl;
-  bool mydup = false;
-  for (int j = 0; j < ns; ++j) {
-    const i32 s = __shfl_sync(FULL, sv, j);
-    int pj = 0;
-    bool eq = false;
+  int rl;
+  bool eqS;
+  if (MR == 1) {
+    const i32 l31 = __shfl_sync(FULL, lr[0], 31);
+    rl = 0;
 #pragma unroll
-    for (int m = 0; m < MR; ++m) {
-      if (32 * m < nl) {
-        pj += __popc(__ballot_sync(FULL, lr[m] < s));
-        eq |= __ballot_sync(FULL, lr[m] == s) != 0;
-      }
+    for (int step = 16; step >= 1; step >>= 1) {
+      const i32 y = __shfl_sync(FULL, lr[0], rl + step - 1);
+      if (y < sv) rl += step;
     }
-    if (lane == j) {
-      mypos = pj;
-      mydup = eq;
+    if (rl == 31 && l31 < sv) rl = 32;
+    const i32 y = __shfl_sync(FULL, lr[0], rl & 31);
+    eqS = lane < ns && rl < nl && y == sv;
+  } else {
+    int lo = 0, hi = lane < ns ? nl : 0;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ld<G>(L + mid) < sv) lo = mid + 1;
+      else hi = mid;
     }
-#pragma unroll
-    for (int m = 0; m < MR; ++m) {
-      const int i = lane + 32 * m;
-      const bool le = pj <= i;
-      c[m] += le;
-      dc[m] += (eq && le);
-      del[m] |= (eq && pj == i);
-    }
+    rl = lo;
+    eqS = lane < ns && rl < nl && ld<G>(L + rl) == sv;
   }
-  const u32 dm = __ballot_sync(FULL, lane < ns && mydup);
-  if (lane < ns && !mydup) out[mypos + lane - 2 * __popc(dm & lt)] = sv;
+  const u32 dmS = __ballot_sync(FULL, eqS);
+  if (lane < ns && !eqS) out[lane + rl - 2 * __popc(dmS & lt)] = sv;
+  int before = 0;
 #pragma unroll
   for (int m = 0; m < MR; ++m) {
     const int i = lane + 32 * m;
-    if (i < nl && !del[m]) out[i + c[m] - 2 * dc[m]] = lr[m];
+    if (i < nl && !eqL[m]) out[i + rs[m] - 2 * (before + __popc(dmL[m] & lt))] = lr[m];
+    before += __popc(dmL[m]);
   }
-  return nl + ns - 2 * __popc(dm);
+  return nl + ns - 2 * __popc(dmS);
 }
 
 // out = L xor S for a sorted list L of distinct ranks and a sorted list S of
@@ -215,12 +231,10 @@ __device__ int warp_xor_tiny(const i32* L, int nl, i32 sv, int ns, i32* out) {
 // output length.
 template <bool G>
 __device__ int warp_xor_small(const i32* L, int nl, i32 sv, int ns, i32* out) {
-  if (ns * ((nl + 31) >> 5) <= 64) {
-    if (nl <= 32) return warp_xor_tiny<G, 1>(L, nl, sv, ns, out);
-    if (nl <= 64) return warp_xor_tiny<G, 2>(L, nl, sv, ns, out);
-    if (nl <= 128) return warp_xor_tiny<G, 4>(L, nl, sv, ns, out);
-    if (nl <= 256) return warp_xor_tiny<G, 8>(L, nl, sv, ns, out);
-  }
+  if (nl <= 32) return warp_xor_tiny<G, 1>(L, nl, sv, ns, out);
+  if (nl <= 64) return warp_xor_tiny<G, 2>(L, nl, sv, ns, out);
+  if (nl <= 128) return warp_xor_tiny<G, 4>(L, nl, sv, ns, out);
+  if (nl <= 256) return warp_xor_tiny<G, 8>(L, nl, sv, ns, out);
   const int lane = threadIdx.x & 31;
   const u32 lt = lanemask_lt();
   const bool act = lane < ns;

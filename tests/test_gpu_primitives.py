@@ -89,3 +89,50 @@ def test_dense_call_over_the_triangle_limit_reports_the_exact_count():
     pts = np.random.default_rng(5).standard_normal((3000, 3)).astype(np.float32)
     with pytest.raises(ValueError, match="Triangle count 4495501000 exceeds max_triangles=10000000"):
         rips_persistence(torch.from_numpy(pts).cuda(), 1e3, max_dim=1)  # complete graph: C(3000, 3)
+
+
+def _kruskal(ei, ej, n):
+    """Forest mask and smallest-vertex labels by Kruskal over the positions."""
+    parent = list(range(n))
+
+    def find(v):
+        while parent[v] != v:
+            parent[v] = parent[parent[v]]
+            v = parent[v]
+        return v
+
+    mask = np.zeros(len(ei), np.uint8)
+    for e, (a, b) in enumerate(zip(ei.tolist(), ej.tolist())):
+        ra, rb = find(a), find(b)
+        if ra != rb:
+            mask[e] = 1
+            parent[max(ra, rb)] = min(ra, rb)
+    comp = np.array([find(v) for v in range(n)], np.int32)
+    return mask, comp
+
+
+@pytest.mark.parametrize("n,E", [(2, 1), (300, 200), (1000, 3000), (5000, 12000), (20000, 30000),
+                                 (29000, 80000), (120000, 400000), (700000, 900000)])
+def test_forest_cluster_and_grid_forms_match_kruskal(n, E):
+    """Every form of the forest kernel (one block for tiny graphs, a thread
+    block cluster with the vertices in distributed shared memory up to about
+    450K vertices, a cooperative grid above) against Kruskal, on random
+    multigraphs with self-loops, repeated pairs, long paths and many
+    components."""
+    from flashph_b200.boruvka import boruvka_mask
+    rng = np.random.default_rng(n + E)
+    ei = rng.integers(0, n, E).astype(np.int32)
+    ej = rng.integers(0, n, E).astype(np.int32)
+    if E > 10:
+        k = E // 10  # a long path in scrambled rank order
+        ei[:k] = np.arange(k) % n
+        ej[:k] = (np.arange(k) + 1) % n
+        perm = rng.permutation(E)
+        ei, ej = ei[perm], ej[perm]
+        ej[::97] = ei[::97]  # self-loops
+    ref_mask, ref_comp = _kruskal(ei, ej, n)
+    mask, comp, (ncomp, status) = boruvka_mask(torch.from_numpy(ei).cuda(), torch.from_numpy(ej).cuda(), n)
+    assert int(status.item()) == 0
+    assert np.array_equal(mask.cpu().numpy(), ref_mask)
+    assert np.array_equal(comp.cpu().numpy(), ref_comp)
+    assert int(ncomp.item()) == int((ref_comp == np.arange(n)).sum())
