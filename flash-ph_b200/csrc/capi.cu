@@ -1,6 +1,8 @@
 // Library-wide C entry points: version, error reporting, launch counting.
 #include <atomic>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -12,15 +14,62 @@ std::atomic<unsigned long long> g_launches{0};
 void record_error(cudaError_t e) { g_last_error = cudaGetErrorString(e); }
 void record_message(const char* msg) { g_last_error = msg; }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// Per-device caches of launch facts that do not change while the process
+// runs (attribute and occupancy queries cost a microsecond or more of host
+// time each, on a path that launches dozens of kernels per call).
+namespace {
+std::mutex g_cache_mu;
+struct FuncFact {
+  int dev;
+  const void* func;
+  int threads;
+  size_t smem;
+  int value;
+};
+std::vector<FuncFact> g_smem_set, g_occ;
+int g_sms[64] = {};
+}  // namespace
+
+int device_sms() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!g_sms[dev]) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    g_sms[dev] = v > 0 ? v : 148;
+  }
+  return g_sms[dev];
+}
+
 cudaError_t allow_dynamic_smem(const void* func) {
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  for (const FuncFact& f : g_smem_set)
+    if (f.dev == dev && f.func == func) return cudaSuccess;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa;
   if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, func);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+  if (e == cudaSuccess) g_smem_set.push_back({dev, func, 0, 0, 1});
   return e;
+}
+
+int occupancy(const void* func, int threads, size_t smem) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  for (const FuncFact& f : g_occ)
+    if (f.dev == dev && f.func == func && f.threads == threads && f.smem == smem) return f.value;
+  int v = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, func, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  g_occ.push_back({dev, func, threads, smem, v});
+  return v;
 }
 }  // namespace ph
 

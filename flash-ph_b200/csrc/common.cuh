@@ -42,6 +42,11 @@ void count_launch();
 // so threads launching the kernel concurrently with different requests
 // cannot lower each other's limit. Returns cudaSuccess or the error.
 cudaError_t allow_dynamic_smem(const void* func);
+// SM count of the current device (cached)
+int device_sms();
+// resident blocks per SM of func at this block size and dynamic shared
+// memory (cached; 0 when the query fails)
+int occupancy(const void* func, int threads, size_t smem);
 
 }  // namespace ph
 

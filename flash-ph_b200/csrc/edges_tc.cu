@@ -889,10 +889,8 @@ extern "C" int ph_batch_edges_enumerate_screened(const float* pts, const ph_clou
     PH_CHECK_LAUNCH();
     return PH_ERR_CUDA;
   }
-  int dev = 0, sms = 148, occ = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tc_edges, TC_THREADS, p.smem);
+  const int sms = ph::device_sms();
+  const int occ = ph::occupancy((const void*)k_tc_edges, TC_THREADS, p.smem);
   if (occ != 1) {
     record_message("ph_batch_edges_enumerate_screened: expected one CTA per SM for the TMEM budget");
     return PH_ERR_CUDA;

@@ -382,10 +382,8 @@ extern "C" int ph_boruvka_mst(const int32_t* edge_i, const int32_t* edge_j, int6
     ph::count_launch();
     k_mst<<<1, MST_NT, 0, s>>>(edge_i, edge_j, E, n, parent, best, mst_mask, comp, ctl, d_status, max_rounds);
   } else {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mst, MST_NT, 0);
+    const int sms = ph::device_sms();
+    const int per_sm = ph::occupancy((const void*)k_mst, MST_NT, 0);
     if (per_sm < 1) return PH_ERR_CUDA;
     const i64 want = (work + MST_NT * 2 - 1) / (MST_NT * 2);
     const int blocks = (int)std::max<i64>(2, std::min<i64>(want, (i64)sms * per_sm));

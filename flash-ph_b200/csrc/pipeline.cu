@@ -12,6 +12,7 @@
 //      tetrahedron count when H2 is asked for
 //   4. the H2 reduction's status and row count
 // The results stay on the device in a ph_result until copied out.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <string>
@@ -27,6 +28,9 @@ struct ph_result {
   int ndim = 0;
   cudaStream_t stream = nullptr;
   int64_t stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // E, T, Q, H1 additions, H2 additions
+  // the run's intermediate buffers, released (stream-ordered) by ph_result_free,
+  // so that the caller's copies of the rows are queued before the frees
+  std::vector<void*> scratch;
 };
 
 namespace {
@@ -51,6 +55,11 @@ struct Arena {
     return static_cast<T*>(p);
   }
   void* bytes(size_t n) { return take<unsigned char>((i64)std::max<size_t>(n, 1)); }
+  // hands the buffers to a result, which frees them later
+  void release_to(ph_result* r) {
+    r->scratch.swap(ptrs);
+    ptrs.clear();
+  }
   ~Arena() {
     for (void* p : ptrs) cudaFreeAsync(p, s);
   }
@@ -109,13 +118,35 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-// copies count int64 values (device) to the pinned slots and waits
+// event per host thread for the readback waits
+cudaEvent_t wait_event() {
+  thread_local cudaEvent_t ev = nullptr;
+  if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) ev = nullptr;
+  return ev;
+}
+
+// copies count int64 values (device) to the pinned slots and waits: polls
+// for up to half a millisecond (the usual wait is a few microseconds, and a
+// blocking wait adds its wake-up latency to every readback), then blocks
 int readback(const int64_t* const* src, int count, int64_t* dst, cudaStream_t s) {
   for (int k = 0; k < count; ++k)
     if (cudaMemcpyAsync(dst + k, src[k], sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
       record_error(cudaGetLastError());
       return PH_ERR_CUDA;
     }
+  cudaEvent_t ev = wait_event();
+  if (ev && cudaEventRecord(ev, s) == cudaSuccess) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      const cudaError_t q = cudaEventQuery(ev);
+      if (q == cudaSuccess) return PH_OK;
+      if (q != cudaErrorNotReady) {
+        record_error(q);
+        return PH_ERR_CUDA;
+      }
+      if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(500)) break;
+    }
+  }
   const cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     record_error(e);
@@ -280,6 +311,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (readback(src, 1, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_mst = (int)(H[0] >> 32);
     if (st_mst) return give_up(fail(st_mst, "ph_boruvka_mst failed"));
+    A.release_to(res);
     *out = res;
     return PH_OK;
   }
@@ -380,6 +412,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   res->nrows[1] = H[1];
   res->stats[3] = H[2];
   if (max_dim == 1) {
+    A.release_to(res);
     *out = res;
     return PH_OK;
   }
@@ -439,6 +472,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   }
   res->nrows[2] = H[2];
   res->stats[4] = H[3];
+  A.release_to(res);
   *out = res;
   return PH_OK;
 }
@@ -466,9 +500,29 @@ extern "C" int ph_result_copy(const ph_result* r, int32_t dim, float* dst, int32
   return PH_OK;
 }
 
+extern "C" int ph_result_copy_all(const ph_result* r, float* dst, int32_t to_host, void* stream) {
+  if (!r) return PH_ERR_ARG;
+  int64_t at = 0;
+  for (int k = 0; k < r->ndim; ++k) {
+    if (r->nrows[k] && !dst) return PH_ERR_ARG;
+    if (r->nrows[k]) {
+      const cudaError_t e = cudaMemcpyAsync(dst + 2 * at, r->rows[k], sizeof(float) * 2 * r->nrows[k],
+                                            to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                            (cudaStream_t)stream);
+      if (e != cudaSuccess) {
+        record_error(e);
+        return PH_ERR_CUDA;
+      }
+    }
+    at += r->nrows[k];
+  }
+  return PH_OK;
+}
+
 extern "C" void ph_result_free(ph_result* r) {
   if (!r) return;
   for (float* p : r->rows)
     if (p) cudaFreeAsync(p, r->stream);
+  for (void* p : r->scratch) cudaFreeAsync(p, r->stream);
   delete r;
 }

@@ -1,6 +1,8 @@
 // Exclusive scan and stable LSD radix sort (see prim.cuh).
 #include "prim.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 
 namespace ph {
@@ -112,6 +114,77 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_down(const In* __restrict__ in
   }
 }
 
+// Single-launch form for scans of up to COOP_MAX_PARTS tiles: every block
+// sums its tiles, a grid barrier, then every block scans the tile sums in
+// shared memory and writes its tiles (one launch instead of three, and no
+// state that needs clearing beforehand).
+constexpr int COOP_MAX_PARTS = 2048;
+
+template <typename In, typename Out>
+__global__ void __launch_bounds__(SCAN_NT) k_scan_coop(const In* __restrict__ in, i64 n, i64 nparts,
+                                                      Out* __restrict__ part, Out* __restrict__ out,
+                                                      const int* active) {
+  if (active && !*active) return;  // the flag is the same for every block
+  __shared__ Out sm[SCAN_NT / 32];
+  __shared__ Out spre[COOP_MAX_PARTS];
+  __shared__ Out tile[SCAN_TILE];
+  cooperative_groups::grid_group g = cooperative_groups::this_grid();
+  for (i64 t = blockIdx.x; t < nparts; t += gridDim.x) {
+    const i64 base = t * SCAN_TILE;
+    Out sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      const i64 i = base + (i64)k * SCAN_NT + threadIdx.x;
+      if (i < n) sum += (Out)in[i];
+    }
+    Out tot;
+    block_excl_scan<Out, SCAN_NT>(sum, sm, &tot);
+    if (threadIdx.x == 0) part[t] = tot;
+  }
+  g.sync();
+  // exclusive scan of all tile sums into shared memory
+  Out carry = 0;
+  for (i64 b0 = 0; b0 < nparts; b0 += SCAN_NT) {
+    const i64 i = b0 + threadIdx.x;
+    const Out v = i < nparts ? __ldcg(part + i) : Out(0);
+    Out tot;
+    const Out ex = block_excl_scan<Out, SCAN_NT>(v, sm, &tot);
+    if (i < nparts) spre[i] = carry + ex;
+    carry += tot;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = carry;
+  __syncthreads();
+  for (i64 t = blockIdx.x; t < nparts; t += gridDim.x) {
+    const i64 base = t * SCAN_TILE;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      const int j = k * SCAN_NT + threadIdx.x;
+      const i64 i = base + j;
+      tile[j] = (i < n) ? (Out)in[i] : Out(0);
+    }
+    __syncthreads();
+    Out loc[SCAN_ITEMS];
+    Out sum = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      loc[k] = sum;
+      sum += tile[threadIdx.x * SCAN_ITEMS + k];
+    }
+    Out tot;
+    const Out ex = block_excl_scan<Out, SCAN_NT>(sum, sm, &tot) + spre[t];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) tile[threadIdx.x * SCAN_ITEMS + k] = ex + loc[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      const int j = k * SCAN_NT + threadIdx.x;
+      const i64 i = base + j;
+      if (i < n) out[i] = tile[j];
+    }
+    __syncthreads();
+  }
+}
+
 template <typename In, typename Out>
 int scan_impl(const In* in, Out* out, i64 n, void* ws, size_t ws_bytes, cudaStream_t s,
               const int* active) {
@@ -125,6 +198,18 @@ int scan_impl(const In* in, Out* out, i64 n, void* ws, size_t ws_bytes, cudaStre
   Carve c(ws, ws_bytes);
   Out* part = c.take<Out>(nparts);
   if (!part) return PH_ERR_ARG;
+  if (nparts <= COOP_MAX_PARTS) {
+    const int per_sm = ph::occupancy((const void*)k_scan_coop<In, Out>, SCAN_NT, 0);
+    const i64 resident = (i64)ph::device_sms() * per_sm;
+    if (resident > 0) {
+      const int grid = (int)std::min<i64>(nparts, resident);
+      void* args[] = {(void*)&in, (void*)&n, (void*)&nparts, (void*)&part, (void*)&out, (void*)&active};
+      ph::count_launch();
+      if (cudaLaunchCooperativeKernel((const void*)k_scan_coop<In, Out>, grid, SCAN_NT, args, 0, s) != cudaSuccess)
+        return PH_ERR_CUDA;
+      return PH_OK;
+    }
+  }
   ph::count_launch();
   k_scan_reduce<In, Out><<<(unsigned)nparts, SCAN_NT, 0, s>>>(in, n, part, active);
   ph::count_launch();
@@ -149,9 +234,13 @@ int scan_impl(const In* in, Out* out, i64 n, void* ws, size_t ws_bytes, cudaStre
 // inclusive prefix. The look-back spin is bounded.
 constexpr int RS_NT = 256;
 constexpr int RS_WARPS = RS_NT / 32;
-constexpr int RS_PER_WARP = 512;
-constexpr int RS_TILE = RS_WARPS * RS_PER_WARP;  // 4096 keys per tile
-constexpr int RS_ROUNDS = RS_PER_WARP / 32;      // 16
+// keys per tile: 8 warps x 32 lanes x ROUNDS. Large sorts take 16 rounds
+// (4096 keys, few look-back slots); sorts of up to RS_SMALL_MAX keys take 4
+// (1024 keys), so that four times as many blocks share the pass and each runs
+// a quarter of the serial counting rounds.
+constexpr int RS_ROUNDS_LARGE = 16, RS_ROUNDS_SMALL = 4;
+constexpr i64 RS_SMALL_MAX = i64(1) << 18;
+__host__ __device__ constexpr int rs_tile(int rounds) { return RS_WARPS * 32 * rounds; }
 constexpr u64 LB_AGG = 1ull << 32, LB_PRE = 2ull << 32;
 constexpr int LB_SPIN_LIMIT = 1 << 24;
 
@@ -209,9 +298,12 @@ __device__ __forceinline__ void pass_plan(const SortCtl* ctl, i64 n, int p0, int
   *count = c;
 }
 
+template <int RS_ROUNDS>
 __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u32* vB, i64 n, int p0,
                                                   int pass, SortCtl* ctl, unsigned long long* lb,
                                                   i64 ntiles) {
+  constexpr int RS_PER_WARP = 32 * RS_ROUNDS;
+  constexpr int RS_TILE = rs_tile(RS_ROUNDS);
   __shared__ u32 tile_sh;
   // the first ticket is taken before the plan so that its latency overlaps it
   if (threadIdx.x == 0) tile_sh = atomicAdd(&ctl->ticket[pass], 1u);
@@ -390,8 +482,13 @@ int scan_exclusive_u8_i32(const uint8_t* in, i32* out, i64 n, void* ws, size_t w
   return scan_impl<uint8_t, i32>(in, out, n, ws, ws_bytes, s, nullptr);
 }
 
+namespace {
+int rs_rounds(i64 n) { return n <= RS_SMALL_MAX ? RS_ROUNDS_SMALL : RS_ROUNDS_LARGE; }
+}  // namespace
+
 size_t radix_sort_workspace_bytes(i64 n) {
-  const i64 ntiles = (n + RS_TILE - 1) / RS_TILE + 1;
+  const i64 tile = rs_tile(rs_rounds(n));
+  const i64 ntiles = (n + tile - 1) / tile + 1;
   return Carve::need((size_t)n * 8) + Carve::need((size_t)n * 4) + Carve::need(sizeof(SortCtl)) +
          Carve::need((size_t)ntiles * 256 * 8);
 }
@@ -402,7 +499,9 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
       begin_bit > end_bit)
     return PH_ERR_ARG;
   if (n <= 1 || begin_bit == end_bit) return PH_OK;
-  const i64 ntiles = (n + RS_TILE - 1) / RS_TILE;
+  const int rounds = rs_rounds(n);
+  const i64 tile = rs_tile(rounds);
+  const i64 ntiles = (n + tile - 1) / tile;
   Carve c(ws, ws_bytes);
   u64* kB = c.take<u64>(n);
   u32* vB = c.take<u32>(n);
@@ -419,7 +518,10 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
   const int gp = (int)std::min<i64>(ntiles, 148 * 4);
   for (int p = p0; p < p1; ++p) {
     ph::count_launch();
-    k_os_pass<<<gp, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
+    if (rounds == RS_ROUNDS_SMALL)
+      k_os_pass<RS_ROUNDS_SMALL><<<gp, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
+    else
+      k_os_pass<RS_ROUNDS_LARGE><<<gp, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
   }
   const int gf = (int)std::max<i64>(1, std::min<i64>((n + 255) / 256, 1184));
   ph::count_launch();

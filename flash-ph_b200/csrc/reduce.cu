@@ -729,11 +729,9 @@ using namespace ph;
 
 // Grid of k_reduce on the current device: persistent blocks, one per resident slot.
 int reduce_blocks(i64 K) {
-  int dev = 0, sms = 148, occ = 1;
   ph::allow_dynamic_smem((const void*)k_reduce);
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_reduce, RD_NT, RD_SMEM);
+  const int sms = ph::device_sms();
+  const int occ = ph::occupancy((const void*)k_reduce, RD_NT, RD_SMEM);
   return (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
 }
 

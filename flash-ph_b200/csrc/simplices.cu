@@ -318,10 +318,8 @@ extern "C" int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx
     PH_CHECK_LAUNCH();
     return PH_ERR_CUDA;
   }
-  int dev = 0, sms = 148, occ = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tri_total, SX_NT, smem);
+  const int sms = ph::device_sms();
+  const int occ = ph::occupancy((const void*)k_tri_total, SX_NT, smem);
   const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
   ph::count_launch();
   k_tri_total<<<grid, SX_NT, smem, s>>>(adj_ptr, adj_idx, n, d_next, d_total);

@@ -122,19 +122,18 @@ def _compute_native(points: Tensor, t: float, max_dim: int, out_device, max_tria
         raise L.PHError("ph_rips_persistence", rc, msg)
     try:
         to_host = out_device.type != "cuda"
-        outs = []
-        for k in range(max_dim + 1):
-            m = int(lib.ph_result_rows(res, k))
-            if to_host:
-                o = torch.empty(m, 2, dtype=torch.float32, pin_memory=True)
-            else:
-                o = torch.empty(m, 2, dtype=torch.float32, device=out_device)
-            L.call("ph_result_copy", res, k, o.data_ptr(), 1 if to_host else 0, s)
-            outs.append(o)
+        rows = [int(lib.ph_result_rows(res, k)) for k in range(max_dim + 1)]
+        # one buffer and one copy call for all diagrams; the diagrams are views of it
         if to_host:
-            torch.cuda.current_stream(dev).synchronize()
+            buf = torch.empty(sum(rows), 2, dtype=torch.float32, pin_memory=True)
+        else:
+            buf = torch.empty(sum(rows), 2, dtype=torch.float32, device=out_device)
+        L.call("ph_result_copy_all", res, buf.data_ptr(), 1 if to_host else 0, s)
+        outs = list(buf.split(rows))
     finally:
         lib.ph_result_free(res)
+    if to_host:
+        torch.cuda.current_stream(dev).synchronize()
     return outs
 
 

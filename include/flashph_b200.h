@@ -307,6 +307,10 @@ int64_t ph_result_rows(const ph_result* result, int32_t dim);
 int64_t ph_result_stat(const ph_result* result, int32_t k);
 /* copies diagram dim (rows x 2 float32) to dst, device or host memory */
 int ph_result_copy(const ph_result* result, int32_t dim, float* dst, int32_t to_host, void* stream);
+/* copies every diagram, dim 0 first, into one buffer of sum(rows) x 2 float32 */
+int ph_result_copy_all(const ph_result* result, float* dst, int32_t to_host, void* stream);
+/* releases the diagrams and the run's intermediate buffers (stream-ordered, on
+ * the stream of the run; call it after the copies are queued) */
 void ph_result_free(ph_result* result);
 
 /* ---- batches of clouds ---------------------------------------------------- */

@@ -136,3 +136,21 @@ def test_forest_cluster_and_grid_forms_match_kruskal(n, E):
     assert np.array_equal(mask.cpu().numpy(), ref_mask)
     assert np.array_equal(comp.cpu().numpy(), ref_comp)
     assert int(ncomp.item()) == int((ref_comp == np.arange(n)).sum())
+
+
+@pytest.mark.parametrize("E", [1, 2047, 2048, 2049, 1 << 20, (1 << 22) + 5])
+def test_h0_rows_through_both_scan_forms(E):
+    """H0 rows place forest edge e at the exclusive prefix count of the mask:
+    the single-launch scan (up to 4M entries) and the three-launch one
+    (above) against numpy, at tile-boundary sizes."""
+    from flashph_b200.boruvka import h0_rows
+    rng = np.random.default_rng(E)
+    n = E + 7
+    mask = (rng.random(E) < 0.3).astype(np.uint8)
+    filt = np.sort(rng.random(E).astype(np.float32))
+    rows = h0_rows(torch.from_numpy(filt).cuda(), torch.from_numpy(mask).cuda(), n).cpu().numpy()
+    k = int(mask.sum())
+    assert rows.shape == (n, 2)
+    assert np.all(rows[:, 0] == 0)
+    assert np.array_equal(rows[:k, 1], filt[mask == 1])
+    assert np.all(np.isinf(rows[k:, 1]))
