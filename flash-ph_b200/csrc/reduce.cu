@@ -150,75 +150,90 @@ __device__ __forceinline__ i32 ld(const i32* p) {
   return *p;
 }
 
-// out = L xor S for L (<= 32 MR entries) and S (ns <= 32, one per lane in sv)
-// with L in registers. An element's output position is its rank in its own
-// list plus its rank in the other list, less twice the common values below
-// it; common values are dropped. Ranks of L entries in S come from a
-// branch-free lower bound over the lanes holding S (five shuffles plus one
-// for the 32nd lane), ranks of S entries in L the same way over L's lanes
-// (MR = 1) or a binary search of L (MR > 1). The searches of the MR chunks are
-// independent, so their latencies overlap.
+// out = L xor S for L (<= 32 MR entries, in registers) and S (ns <= 32, one
+// per lane in sv). An element's output position is its rank in its own list
+// plus its rank in the other list, less twice the common values below it;
+// common values are dropped. The ranks of L's entries in S come from ns
+// broadcasts of S (independent shuffles, so their latencies overlap). L being
+// sorted, those ranks are non-decreasing, and the S entries that fall between
+// L[i-1] and L[i] are exactly S[rank(L[i-1]) ..< rank(L[i])] (past a common
+// value): the lane holding L[i] writes them, knowing their rank in L (i)
+// without any search. S entries above all of L are written by their own lanes.
 template <bool G, int MR>
 __device__ int warp_xor_tiny(const i32* L, int nl, i32 sv, int ns, i32* out) {
   const int lane = threadIdx.x & 31;
   const u32 lt = lanemask_lt();
   i32 lr[MR];
-#pragma unroll
-  for (int m = 0; m < MR; ++m) lr[m] = (lane + 32 * m < nl) ? ld<G>(L + lane + 32 * m) : INT_MAX;
-  const i32 s31 = __shfl_sync(FULL, sv, 31);
   int rs[MR];
-#pragma unroll
-  for (int m = 0; m < MR; ++m) rs[m] = 0;
-#pragma unroll
-  for (int step = 16; step >= 1; step >>= 1) {
-#pragma unroll
-    for (int m = 0; m < MR; ++m) {
-      const i32 y = __shfl_sync(FULL, sv, rs[m] + step - 1);
-      if (y < lr[m]) rs[m] += step;
-    }
-  }
-  bool eqL[MR];
-  u32 dmL[MR];
+  bool eq[MR], valid[MR];
 #pragma unroll
   for (int m = 0; m < MR; ++m) {
-    if (rs[m] == 31 && s31 < lr[m]) rs[m] = 32;
-    const i32 y = __shfl_sync(FULL, sv, rs[m] & 31);
-    eqL[m] = lane + 32 * m < nl && rs[m] < ns && y == lr[m];
-    dmL[m] = __ballot_sync(FULL, eqL[m]);
+    valid[m] = lane + 32 * m < nl;
+    lr[m] = valid[m] ? ld<G>(L + lane + 32 * m) : INT_MAX;
+    rs[m] = 0;
+    eq[m] = false;
   }
-  int rl;
-  bool eqS;
-  if (MR == 1) {
-    const i32 l31 = __shfl_sync(FULL, lr[0], 31);
-    rl = 0;
+  for (int j0 = 0; j0 < ns; j0 += 8) {  // eight broadcasts in flight at a time
+    i32 s[8];
 #pragma unroll
-    for (int step = 16; step >= 1; step >>= 1) {
-      const i32 y = __shfl_sync(FULL, lr[0], rl + step - 1);
-      if (y < sv) rl += step;
-    }
-    if (rl == 31 && l31 < sv) rl = 32;
-    const i32 y = __shfl_sync(FULL, lr[0], rl & 31);
-    eqS = lane < ns && rl < nl && y == sv;
-  } else {
-    int lo = 0, hi = lane < ns ? nl : 0;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (ld<G>(L + mid) < sv) lo = mid + 1;
-      else hi = mid;
-    }
-    rl = lo;
-    eqS = lane < ns && rl < nl && ld<G>(L + rl) == sv;
+    for (int q = 0; q < 8; ++q) s[q] = __shfl_sync(FULL, sv, (j0 + q) & 31);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (j0 + q < ns) {
+#pragma unroll
+        for (int m = 0; m < MR; ++m) {
+          rs[m] += s[q] < lr[m];
+          eq[m] |= s[q] == lr[m];
+        }
+      }
   }
-  const u32 dmS = __ballot_sync(FULL, eqS);
-  if (lane < ns && !eqS) out[lane + rl - 2 * __popc(dmS & lt)] = sv;
-  int before = 0;
+  u32 dm[MR];
+  int before[MR];
+  int dtot = 0;
+#pragma unroll
+  for (int m = 0; m < MR; ++m) {
+    dm[m] = __ballot_sync(FULL, eq[m] && valid[m]);
+    before[m] = dtot;
+    dtot += __popc(dm[m]);
+  }
+  // L's entries
+  int lo[MR], span = 0;
 #pragma unroll
   for (int m = 0; m < MR; ++m) {
     const int i = lane + 32 * m;
-    if (i < nl && !eqL[m]) out[i + rs[m] - 2 * (before + __popc(dmL[m] & lt))] = lr[m];
-    before += __popc(dmL[m]);
+    const int d = before[m] + __popc(dm[m] & lt);
+    if (valid[m] && !eq[m]) out[i + rs[m] - 2 * d] = lr[m];
+    // first S index after L[i-1] (past it when they are equal)
+    int prev = __shfl_up_sync(FULL, rs[m] + (int)eq[m], 1);
+    if (m > 0) {
+      const int last = __shfl_sync(FULL, rs[m - 1] + (int)eq[m - 1], 31);
+      if (lane == 0) prev = last;
+    } else if (lane == 0) {
+      prev = 0;
+    }
+    lo[m] = prev;
+    if (valid[m]) span = max(span, rs[m] - lo[m]);
   }
-  return nl + ns - 2 * __popc(dmS);
+  span = __reduce_max_sync(FULL, span);
+  // S entries between L[i-1] and L[i], written by the lane holding L[i]
+  for (int t = 0; t < span; ++t) {
+#pragma unroll
+    for (int m = 0; m < MR; ++m) {
+      const int j = lo[m] + t;
+      const i32 v = __shfl_sync(FULL, sv, j & 31);
+      if (valid[m] && j < rs[m]) out[j + lane + 32 * m - 2 * (before[m] + __popc(dm[m] & lt))] = v;
+    }
+  }
+  // S entries above all of L
+  int lo_end = 0;
+  if (nl > 0) {
+    const int ml = (nl - 1) >> 5, ll = (nl - 1) & 31;
+#pragma unroll
+    for (int m = 0; m < MR; ++m)
+      if (m == ml) lo_end = __shfl_sync(FULL, rs[m] + (int)eq[m], ll);
+  }
+  if (lane < ns && lane >= lo_end) out[lane + nl - 2 * dtot] = sv;
+  return nl + ns - 2 * dtot;
 }
 
 // out = L xor S for a sorted list L of distinct ranks and a sorted list S of
@@ -407,28 +422,74 @@ __device__ __forceinline__ unsigned long long pool_alloc(PoolChunk& ch, RedCtl* 
 }
 
 // ---- dense working columns ---------------------------------------------------------
-// A working column longer than the shared buffer becomes a bitmap over the
-// row range in global memory, private to its warp (one slot per warp of the
-// grid, cleared on first use and after each column): adding a column flips
-// its bits, the next pivot is the first set bit at or after the current one
-// (the added column's entries are all >= the pivot it cancels), and the
-// sorted record is produced only when the column claims a pivot. Cost per
-// addition is the added column's length, not the working column's.
+// A working column can be a bitmap over the row range, private to its warp
+// (cleared on first use and after each column): adding a column flips its
+// bits, the next pivot is the first set bit at or after the current one (the
+// added column's entries are all >= the pivot it cancels), and the sorted
+// record is produced only when the column claims a pivot. Cost per addition
+// is the added column's length, not the working column's. When the row range
+// fits one of the warp's shared buffers (up to 32 * RD_CAP rows) every
+// working column is such a bitmap in shared memory; otherwise only a column
+// that outgrows its shared buffer becomes one, in a global slot per warp.
 struct DenseCol {
-  u32* bits = nullptr;  // this warp's slot
+  u32* bits = nullptr;  // this warp's bitmap
   i64 lo = 0, hi = -1;  // touched word range
   i32 piv = -1;         // lowest set bit (global rank)
+  bool sm = false;      // bits are in this warp's shared memory
 };
+
+// shared-memory forms of the bitmap accesses (explicit state space: the
+// bitmap pointer is generic, and generic atomics and loads take a slower path)
+__device__ __forceinline__ u32 sm_ld32(const u32* p) {
+  u32 v;
+  asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"((u32)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ u32 sm_xor32(u32* p, u32 x) {
+  u32 old;
+  asm volatile("atom.shared.xor.b32 %0, [%1], %2;" : "=r"(old) : "r"((u32)__cvta_generic_to_shared(p)), "r"(x)
+               : "memory");
+  return old;
+}
+__device__ __forceinline__ void sm_st32(u32* p, u32 v) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ u32 dense_word(const DenseCol& D, i64 w) { return D.sm ? sm_ld32(D.bits + w) : __ldcg(D.bits + w); }
+__device__ __forceinline__ u32 dense_xor(const DenseCol& D, i64 w, u32 b) {
+  return D.sm ? sm_xor32(D.bits + w, b) : atomicXor(D.bits + w, b);
+}
 
 // flips the sorted entries src[0..len) (global ranks); returns the change in
 // the number of set bits (warp-uniform) and widens the touched range
+// flips the sorted entries held one per lane (lanes < len <= 32)
+__device__ int dense_flip_regs(DenseCol& D, i32 v, int len, i32 row_base) {
+  const int lane = threadIdx.x & 31;
+  int delta = 0;
+  if (lane < len) {
+    const i32 e = v - row_base;
+    const u32 b = 1u << (e & 31);
+    const u32 old = dense_xor(D, e >> 5, b);
+    delta = (old & b) ? -1 : 1;
+  }
+  delta = __reduce_add_sync(FULL, delta);
+  const i32 first = __shfl_sync(FULL, v, 0), last = __shfl_sync(FULL, v, (len - 1) & 31);
+  if (len > 0) {
+    const i64 w0 = (i64)((first - row_base) >> 5), w1 = (i64)((last - row_base) >> 5);
+    D.lo = D.hi < D.lo ? w0 : min(D.lo, w0);
+    D.hi = max(D.hi, w1);
+  }
+  __syncwarp();
+  return delta;
+}
+
 __device__ int dense_flip(DenseCol& D, const i32* src, bool srcg, int len, i32 row_base) {
   const int lane = threadIdx.x & 31;
   int delta = 0;
   for (int i = lane; i < len; i += 32) {
     const i32 e = (srcg ? __ldcg(src + i) : src[i]) - row_base;
     const u32 b = 1u << (e & 31);
-    const u32 old = atomicXor(D.bits + (e >> 5), b);
+    const u32 old = dense_xor(D, e >> 5, b);
     delta += (old & b) ? -1 : 1;
   }
   delta = __reduce_add_sync(FULL, delta);
@@ -447,7 +508,7 @@ __device__ i32 dense_first(const DenseCol& D, i64 from, i32 row_base) {
   const int lane = threadIdx.x & 31;
   for (i64 w0 = from; w0 <= D.hi; w0 += 32) {
     const i64 w = w0 + lane;
-    const u32 v = w <= D.hi ? __ldcg(D.bits + w) : 0u;
+    const u32 v = w <= D.hi ? dense_word(D, w) : 0u;
     const u32 m = __ballot_sync(FULL, v != 0);
     if (m) {
       const int f = __ffs(m) - 1;
@@ -464,7 +525,7 @@ __device__ void dense_to_list(const DenseCol& D, i32 row_base, i32* out) {
   int pos = 0;
   for (i64 w0 = (i64)((D.piv - row_base) >> 5); w0 <= D.hi; w0 += 32) {
     const i64 w = w0 + lane;
-    u32 v = w <= D.hi ? __ldcg(D.bits + w) : 0u;
+    u32 v = w <= D.hi ? dense_word(D, w) : 0u;
     const int c = __popc(v);
     int incl = c;
 #pragma unroll
@@ -484,7 +545,10 @@ __device__ void dense_to_list(const DenseCol& D, i32 row_base, i32* out) {
 
 __device__ void dense_clear(DenseCol& D, i64 lo, i64 hi) {
   const int lane = threadIdx.x & 31;
-  for (i64 w = lo + lane; w <= hi; w += 32) __stcg(D.bits + w, 0u);
+  if (D.sm)
+    for (i64 w = lo + lane; w <= hi; w += 32) sm_st32(D.bits + w, 0u);
+  else
+    for (i64 w = lo + lane; w <= hi; w += 32) __stcg(D.bits + w, 0u);
   __syncwarp();
   D.lo = 0;
   D.hi = -1;
@@ -494,10 +558,10 @@ __device__ void dense_clear(DenseCol& D, i64 lo, i64 hi) {
 // Residual columns are taken in descending order (the serial algorithm's
 // order), RD_FETCH at a time per warp, so that a column mostly meets final
 // versions of the larger columns it adds and is rarely displaced.
-__global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32* __restrict__ state,
+__global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const i32* __restrict__ state,
                                                  const u64* __restrict__ rec, u64* owner, i32* pool, i64 pool_cap,
                                                  int chunk, RedCtl* ctl, int* status, int max_steps,
-                                                 u32* dense_bits, i64 dense_words) {
+                                                 u32* dense_bits, i64 dense_words, int sm_words) {
   extern __shared__ i32 rd_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   i32* const sW0 = rd_smem + (size_t)w * RD_WSTRIDE;  // working copies at sW0 and sW0 + RD_CAP
@@ -507,8 +571,16 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
   unsigned long long n_merges = 0, n_takeovers = 0;
   DenseCol D;
   bool dense_ready = false;  // this warp's slot has been cleared once
-  const bool dense_ok = dense_words > 0;
-  if (dense_ok) D.bits = dense_bits + (size_t)(blockIdx.x * RD_WARPS + w) * (size_t)dense_words;
+  // shared bitmap (in the second working buffer) when the rows fit, else the global slot
+  const bool dense_sm = sm_words > 0;
+  const bool dense_ok = dense_sm || dense_words > 0;
+  const i64 dwords = dense_sm ? (i64)sm_words : dense_words;
+  if (dense_sm) {
+    D.bits = reinterpret_cast<u32*>(sW0 + RD_CAP);
+    D.sm = true;
+  } else if (dense_ok) {
+    D.bits = dense_bits + (size_t)(blockIdx.x * RD_WARPS + w) * (size_t)dense_words;
+  }
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&ctl->next, RD_FETCH);
@@ -530,11 +602,11 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
     bool dense = false;   // W is the bitmap D
     auto enter_dense = [&](const i32* src, bool srcg, int len) {
       if (!dense_ready) {
-        dense_clear(D, 0, dense_words - 1);
+        dense_clear(D, 0, dwords - 1);
         dense_ready = true;
       }
       dense_flip(D, src, srcg, len, row_base);
-      D.piv = srcg ? __ldcg(src) : src[0];
+      D.piv = len > 0 ? (srcg ? __ldcg(src) : src[0]) : -1;
       dense = true;
     };
     auto leave_dense = [&]() {
@@ -544,7 +616,7 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
     auto load_record = [&](u64 at) {
       const i32* src = pool + at + 1;
       k = __ldcg(pool + at);
-      if (k > RD_CAP && dense_ok) {
+      if (dense_sm || (k > RD_CAP && dense_ok)) {
         enter_dense(src, true, k);
       } else if (k <= RD_CAP) {
         for (int i = lane; i < k; i += 32) (sW0 + cur * RD_CAP)[i] = __ldcg(src + i);
@@ -559,18 +631,29 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
       published = true;
     };
     load_record(rec[c]);
+    // After a takeover the working column still holds the content of the
+    // column that just claimed the pivot, and the displaced column must add
+    // exactly that content: the step adds the displaced record to it instead
+    // of loading the displaced record and then re-reading the owner word and
+    // the record just published (two fewer dependent L2 round trips on the
+    // takeover chains that form the critical path).
+    u64 pending = 0;
     for (int step = 0;; ++step) {
-      if (step > 0 && dense && *vabort) break;
+      // another warp's abort (pool exhausted) is checked every 64 steps: the
+      // flag is an L2 round trip, as long as a whole step of a short column
+      if (dense && (step & 63) == 63 && *vabort) break;
       if (step >= max_steps) {
         if (lane == 0) set_status(status, PH_ERR_ITER_LIMIT);
         atomicExch(&ctl->abort, 1);
         break;
       }
       if (k == 0) break;  // the column vanished: it owns nothing
+      const bool take = pending != 0;
       const i32 p = dense ? D.piv : (wg ? __ldcg(W) : W[0]);
-      u64 ow = ld_acquire(owner + (p - row_base));
+      u64 ow = take ? pending : ld_acquire(owner + (p - row_base));
+      pending = 0;
       i32 o = owner_col(ow);
-      if (o < c) {
+      if (!take && o < c) {
         // publish W as a record, then claim p
         if (!published) {
           const unsigned long long at = pool_alloc(chunk_state, ctl, pool_cap, k + 1, chunk, status);
@@ -590,18 +673,38 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
         __syncwarp();
         const i32 oc = owner_col(old);
         if (oc < c) {
-          leave_dense();
-          if (oc < 0) break;  // claimed a free pivot: this work item is done
+          if (oc < 0) {  // claimed a free pivot: this work item is done
+            leave_dense();
+            break;
+          }
           // displaced a smaller column: take it over
           ++n_takeovers;
           c = oc;
+          if (dense) {
+            // the bitmap holds the claimer's content: flip the displaced record into it
+            const u64 at_d = old & OW_OFF;
+            const int len_d = __ldcg(pool + at_d);
+            k += dense_flip(D, pool + at_d + 1, true, len_d, row_base);
+            ++n_merges;
+            published = false;
+            if (k == 0) {
+              leave_dense();
+              break;
+            }
+            D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+            continue;
+          }
+          if (!wg) {
+            pending = old;  // next step: W (the claimer's content) + the displaced record
+            continue;
+          }
           load_record(old & OW_OFF);
           continue;
         }
         o = oc;  // a larger column got there first
         ow = old;
       }
-      if (o == c) {  // cannot happen: a column never owns a pivot it is still reducing
+      if (!take && o == c) {  // cannot happen: a column never owns a pivot it is still reducing
         if (lane == 0) set_status(status, PH_ERR_ARG);
         break;
       }
@@ -612,7 +715,8 @@ __global__ void __launch_bounds__(RD_NT) k_reduce(i32 row_base, i64 K, const i32
       const i32 bv = __shfl_down_sync(FULL, head, 1);  // entry `lane` of B (lanes < 31)
       if (!dense && dense_ok && k + lb > RD_CAP) enter_dense(W, wg, k);  // W outgrows its buffer
       if (dense) {
-        k += dense_flip(D, pool + at_o + 1, true, lb, row_base);
+        // entries 0..30 of the added column are already in registers
+        k += lb <= 31 ? dense_flip_regs(D, bv, lb, row_base) : dense_flip(D, pool + at_o + 1, true, lb, row_base);
         ++n_merges;
         published = false;
         if (k == 0) {
@@ -735,9 +839,18 @@ int reduce_blocks(i64 K) {
   return (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
 }
 
-// dense working-column slots: one bitmap of R bits per warp of the grid, when
-// they fit in 1 GiB (else long columns stay sorted lists in the pool)
+// words of the shared-memory bitmap each warp uses for every working column,
+// 0 when R rows do not fit one working buffer
+int sm_dense_words(i64 R) {
+  const i64 words = (R + 31) / 32 + 1;
+  return words <= RD_CAP ? (int)words : 0;
+}
+
+// dense working-column slots in global memory (rows beyond the shared bitmap):
+// one bitmap of R bits per warp of the grid, when they fit in 1 GiB (else long
+// columns stay sorted lists in the pool)
 i64 dense_words(i64 K, i64 R) {
+  if (sm_dense_words(R)) return 0;
   const i64 words = (R + 31) / 32 + 1;
   const i64 warps = (i64)reduce_blocks(K) * RD_WARPS;
   return words * warps * 4 <= (i64(1) << 30) ? words : 0;
@@ -785,7 +898,7 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   const int chunk = (int)std::max<i64>(64, std::min<i64>(2048, pool_cap / (4 * (i64)blocks * RD_WARPS)));
   ph::count_launch();
   k_reduce<<<blocks, RD_NT, RD_SMEM, s>>>(row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
-                                          1 << 24, dense, dw);
+                                          1 << 24, dense, dw, sm_dense_words(R));
   ph::count_launch();
   k_finish_cols<<<grid_for(K), 256, 0, s>>>(K, col_state, col_piv, ctl, d_info);
   if (R > 0) {
