@@ -499,7 +499,7 @@ def kernel_breakdown(pts, t, max_dim, flush, reps=3):
 # DRAM traffic per launch from ncu captures of this workload (profiles/*.md)
 NCU_TRAFFIC = {
     "k_tc_edges": {"bytes": 2.29e6 + 0.02e6, "source": "profiles/k_tc_edges_20k_d10.md"},
-    "k_reduce": {"bytes": 0.87e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
+    "k_reduce": {"bytes": 0.83e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
 }
 
 
