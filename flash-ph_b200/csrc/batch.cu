@@ -37,6 +37,8 @@ __device__ __forceinline__ int seg_of(const i64* __restrict__ off, int nsegs, i6
 }
 
 __global__ void k_vertex_cloud(const ph_cloud_seg* __restrict__ segs, int nsegs, i32* __restrict__ vcloud) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (int c = blockIdx.x; c < nsegs; c += gridDim.x)
     for (i64 v = threadIdx.x; v < segs[c].n; v += blockDim.x) vcloud[segs[c].vbase + v] = c;
 }
@@ -45,6 +47,8 @@ __global__ void k_vertex_cloud(const ph_cloud_seg* __restrict__ segs, int nsegs,
 __global__ void k_local_keys(const i32* __restrict__ ei, const i32* __restrict__ ej, const float* __restrict__ dsq,
                              i64 E, const i32* __restrict__ vcloud, const ph_cloud_seg* __restrict__ segs,
                              u64* __restrict__ keys, u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     const i32 c = vcloud[ei[e]];
     const u64 vb = (u64)segs[c].vbase;
@@ -57,6 +61,8 @@ __global__ void k_local_keys(const i32* __restrict__ ei, const i32* __restrict__
 
 __global__ void k_cloud_keys(const u32* __restrict__ perm, const i32* __restrict__ ei, i64 E,
                              const i32* __restrict__ vcloud, u64* __restrict__ keys, u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x; k < E; k += (i64)gridDim.x * blockDim.x) {
     const u32 e = perm[k];
     keys[k] = (u64)(u32)vcloud[ei[e]];
@@ -86,6 +92,8 @@ __device__ __forceinline__ u64 emission_order_local(u32 e, const i32* ei, const 
 __global__ void k_fix_ties_batch(u32* __restrict__ vals, i64 E, const i32* __restrict__ ei,
                                  const i32* __restrict__ ej, const float* __restrict__ dsq,
                                  const i32* __restrict__ vcloud, const ph_cloud_seg* __restrict__ segs) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < E; p += (i64)gridDim.x * blockDim.x) {
     const u32 ep = vals[p];
     const i32 cp = vcloud[ei[ep]];
@@ -113,6 +121,8 @@ __global__ void k_fix_ties_batch(u32* __restrict__ vals, i64 E, const i32* __res
 __global__ void k_gather3(const u32* __restrict__ perm, const i32* __restrict__ ei, const i32* __restrict__ ej,
                           const float* __restrict__ dsq, i64 E, i32* __restrict__ oi, i32* __restrict__ oj,
                           float* __restrict__ od) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     const u32 s = perm[e];
     oi[e] = ei[s];
@@ -124,6 +134,8 @@ __global__ void k_gather3(const u32* __restrict__ perm, const i32* __restrict__ 
 // off[c] = first item of cloud c (items grouped by cloud), off[nsegs] = n.
 __global__ void k_item_offsets(const i32* __restrict__ item_vertex, i64 n, const i32* __restrict__ vcloud,
                                int nsegs, i64* __restrict__ off) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   if (n == 0) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= nsegs; c += gridDim.x * blockDim.x) off[c] = 0;
     return;
@@ -141,6 +153,8 @@ __global__ void k_item_offsets(const i32* __restrict__ item_vertex, i64 n, const
 __global__ void k_h0_batch_edges(const float* __restrict__ filt, const uint8_t* __restrict__ mst,
                                  const i32* __restrict__ pos, i64 E, const i64* __restrict__ eoff, int nsegs,
                                  const ph_cloud_seg* __restrict__ segs, float* __restrict__ rows) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     if (!mst[e]) continue;
     const int c = seg_of(eoff, nsegs, e);
@@ -153,6 +167,8 @@ __global__ void k_h0_batch_edges(const float* __restrict__ filt, const uint8_t* 
 __global__ void k_h0_batch_inf(const i32* __restrict__ pos, const i64* __restrict__ eoff, int nsegs,
                                const ph_cloud_seg* __restrict__ segs, const i32* __restrict__ vcloud, i64 N,
                                float* __restrict__ rows) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (i64)gridDim.x * blockDim.x) {
     const int c = vcloud[r];
     const i64 k = r - segs[c].vbase;
@@ -180,6 +196,8 @@ __device__ __forceinline__ bool row_kept(i64 c, const i32* state, const i32* piv
 __global__ void k_rows_flags(const i32* __restrict__ state, const i32* __restrict__ piv, i64 K, i32 row_base,
                              const float* __restrict__ filt, const i32* __restrict__ col_m,
                              const i32* __restrict__ row_m, uint8_t* __restrict__ kept) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x)
     kept[c] = row_kept(c, state, piv, row_base, filt, col_m, row_m) ? 1 : 0;
 }
@@ -195,6 +213,8 @@ __global__ void k_rows_write(const i32* __restrict__ state, const i32* __restric
                              const i32* __restrict__ row_m, const uint8_t* __restrict__ kept,
                              const i32* __restrict__ pos, const i64* __restrict__ col_off, int nsegs,
                              float* __restrict__ rows) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x) {
     const int s = col_off ? seg_of(col_off, nsegs, c) : 0;
     const i64 s0 = col_off ? col_off[s] : 0, s1 = col_off ? col_off[s + 1] : K;
@@ -218,6 +238,8 @@ __global__ void k_rows_write(const i32* __restrict__ state, const i32* __restric
 
 __global__ void k_rows_offsets(const i32* __restrict__ pos, i64 K, const i64* __restrict__ col_off, int nsegs,
                                i64* __restrict__ row_off, i64* __restrict__ d_nrows) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s <= nsegs; s += gridDim.x * blockDim.x)
     if (row_off) row_off[s] = pos[col_off ? col_off[s] : (s ? K : 0)];
   if (blockIdx.x == 0 && threadIdx.x == 0 && d_nrows) *d_nrows = pos[K];
@@ -226,12 +248,16 @@ __global__ void k_rows_offsets(const i32* __restrict__ pos, i64 K, const i64* __
 // ---- masks -----------------------------------------------------------------------
 __global__ void k_edge_dim_mask(const i32* __restrict__ ei, i64 E, const i32* __restrict__ vcloud,
                                 const ph_cloud_seg* __restrict__ segs, int min_dim, uint8_t* __restrict__ out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x)
     out[e] = segs[vcloud[ei[e]]].max_dim >= min_dim ? 1 : 0;
 }
 
 __global__ void k_or_gather(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, const i32* __restrict__ idx,
                             i64 n, int invert) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
     const uint8_t v = src[idx[i]];
     dst[i] |= invert ? (uint8_t)!v : v;
@@ -247,6 +273,8 @@ __global__ void __launch_bounds__(KN_NT) k_knn_batch(const float* __restrict__ p
                                                     const ph_cloud_seg* __restrict__ segs, int nsegs,
                                                     const i64* __restrict__ qb_off, int kreq,
                                                     float* __restrict__ out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   extern __shared__ float sm[];
   const int c = seg_of(qb_off, nsegs, (i64)blockIdx.x);
   const ph_cloud_seg sg = segs[c];
@@ -292,6 +320,8 @@ __global__ void __launch_bounds__(KN_NT) k_knn_batch(const float* __restrict__ p
 
 __global__ void k_seg_value_keys(const float* __restrict__ v, i64 N, const i32* __restrict__ vcloud,
                                  u64* __restrict__ keys, u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (i64)gridDim.x * blockDim.x) {
     u32 b = __float_as_uint(v[i]);
     b = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
@@ -309,6 +339,8 @@ __device__ __forceinline__ float unflip(u64 key) {
 // torch.quantile (linear) per cloud on the cloud's sorted values.
 __global__ void k_seg_quantile(const u64* __restrict__ sorted, const ph_cloud_seg* __restrict__ segs, int nsegs,
                                float qf, float* __restrict__ out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nsegs; c += gridDim.x * blockDim.x) {
     const i64 n = segs[c].n;
     if (n <= 1) {
@@ -341,16 +373,16 @@ int rows_nosort(const i32* state, const i32* piv, i64 K, i32 row_base, const flo
   if (!kept || !pos || !sws) return PH_ERR_ARG;
   if (K > 0) {
     ph::count_launch();
-    k_rows_flags<<<grid_for(K), 256, 0, s>>>(state, piv, K, row_base, filt, col_m, row_m, kept);
+    ph::launch_pdl(k_rows_flags, dim3(grid_for(K)), dim3(256), 0, s, state, piv, K, row_base, filt, col_m, row_m, kept);
   }
   PH_TRY(scan_exclusive_u8_i32(kept, pos, K, sws, scan_workspace_bytes(K), s));
   if (K > 0) {
     ph::count_launch();
-    k_rows_write<<<grid_for(K), 256, 0, s>>>(state, piv, K, row_base, filt, col_m, row_m, kept, pos, col_off,
+    ph::launch_pdl(k_rows_write, dim3(grid_for(K)), dim3(256), 0, s, state, piv, K, row_base, filt, col_m, row_m, kept, pos, col_off,
                                              nsegs, out_rows);
   }
   ph::count_launch();
-  k_rows_offsets<<<1, 256, 0, s>>>(pos, K, col_off, nsegs, row_off, d_nrows);
+  ph::launch_pdl(k_rows_offsets, dim3(1), dim3(256), 0, s, pos, K, col_off, nsegs, row_off, d_nrows);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -367,7 +399,7 @@ extern "C" int ph_batch_vertex_cloud(const ph_cloud_seg* segs, int32_t nsegs, in
   if (nsegs < 0) return PH_ERR_ARG;
   if (nsegs == 0) return PH_OK;
   ph::count_launch();
-  k_vertex_cloud<<<std::min(nsegs, 4096), 256, 0, (cudaStream_t)stream>>>(segs, nsegs, vcloud);
+  ph::launch_pdl(k_vertex_cloud, dim3(std::min(nsegs, 4096)), dim3(256), 0, (cudaStream_t)stream, segs, nsegs, vcloud);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -391,17 +423,17 @@ extern "C" int ph_batch_edges_sort(const int32_t* in_i, const int32_t* in_j, con
   void* rws = c.take<char>((i64)radix_sort_workspace_bytes(E));
   if (!k1 || !v1 || !k2 || !v2 || !rws) return PH_ERR_ARG;
   ph::count_launch();
-  k_local_keys<<<grid_for(E), 256, 0, s>>>(in_i, in_j, in_dsq, E, vcloud, segs, k1, v1);
+  ph::launch_pdl(k_local_keys, dim3(grid_for(E)), dim3(256), 0, s, in_i, in_j, in_dsq, E, vcloud, segs, k1, v1);
   PH_TRY(radix_sort_pairs(k1, v1, E, 0, 64, rws, radix_sort_workspace_bytes(E), s));
   ph::count_launch();
-  k_cloud_keys<<<grid_for(E), 256, 0, s>>>(v1, in_i, E, vcloud, k2, v2);
+  ph::launch_pdl(k_cloud_keys, dim3(grid_for(E)), dim3(256), 0, s, v1, in_i, E, vcloud, k2, v2);
   PH_TRY(radix_sort_pairs(k2, v2, E, 0, 32, rws, radix_sort_workspace_bytes(E), s));
   if (any_wrap) {
     ph::count_launch();
-    k_fix_ties_batch<<<grid_for(E), 256, 0, s>>>(v2, E, in_i, in_j, in_dsq, vcloud, segs);
+    ph::launch_pdl(k_fix_ties_batch, dim3(grid_for(E)), dim3(256), 0, s, v2, E, in_i, in_j, in_dsq, vcloud, segs);
   }
   ph::count_launch();
-  k_gather3<<<grid_for(E), 256, 0, s>>>(v2, in_i, in_j, in_dsq, E, out_i, out_j, out_dsq);
+  ph::launch_pdl(k_gather3, dim3(grid_for(E)), dim3(256), 0, s, v2, in_i, in_j, in_dsq, E, out_i, out_j, out_dsq);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -410,7 +442,7 @@ extern "C" int ph_batch_item_offsets(const int32_t* item_vertex, int64_t n_items
                                      int32_t nsegs, int64_t* off, void* stream) {
   if (n_items < 0 || nsegs < 1) return PH_ERR_ARG;
   ph::count_launch();
-  k_item_offsets<<<grid_for(std::max<i64>(n_items, nsegs + 1)), 256, 0, (cudaStream_t)stream>>>(
+  ph::launch_pdl(k_item_offsets, dim3(grid_for(std::max<i64>(n_items, nsegs + 1))), dim3(256), 0, (cudaStream_t)stream, 
       item_vertex, n_items, vcloud, nsegs, off);
   PH_CHECK_LAUNCH();
   return PH_OK;
@@ -432,11 +464,11 @@ extern "C" int ph_batch_h0_rows(const float* edge_filt, const uint8_t* mst_mask,
   PH_TRY(scan_exclusive_u8_i32(mst_mask, pos, E, sws, scan_workspace_bytes(E), s));
   if (E > 0) {
     ph::count_launch();
-    k_h0_batch_edges<<<grid_for(E), 256, 0, s>>>(edge_filt, mst_mask, pos, E, edge_off, nsegs, segs, out_rows);
+    ph::launch_pdl(k_h0_batch_edges, dim3(grid_for(E)), dim3(256), 0, s, edge_filt, mst_mask, pos, E, edge_off, nsegs, segs, out_rows);
   }
   if (N > 0) {
     ph::count_launch();
-    k_h0_batch_inf<<<grid_for(N), 256, 0, s>>>(pos, edge_off, nsegs, segs, vcloud, N, out_rows);
+    ph::launch_pdl(k_h0_batch_inf, dim3(grid_for(N)), dim3(256), 0, s, pos, edge_off, nsegs, segs, vcloud, N, out_rows);
   }
   PH_CHECK_LAUNCH();
   return PH_OK;
@@ -460,7 +492,7 @@ extern "C" int ph_batch_edge_dim_mask(const int32_t* edge_i, int64_t E, const in
   if (E < 0) return PH_ERR_ARG;
   if (E == 0) return PH_OK;
   ph::count_launch();
-  k_edge_dim_mask<<<grid_for(E), 256, 0, (cudaStream_t)stream>>>(edge_i, E, vcloud, segs, min_dim, out);
+  ph::launch_pdl(k_edge_dim_mask, dim3(grid_for(E)), dim3(256), 0, (cudaStream_t)stream, edge_i, E, vcloud, segs, min_dim, out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -470,7 +502,7 @@ extern "C" int ph_or_gather_mask(uint8_t* dst, const uint8_t* src, const int32_t
   if (n < 0) return PH_ERR_ARG;
   if (n == 0) return PH_OK;
   ph::count_launch();
-  k_or_gather<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(dst, src, idx, n, invert);
+  ph::launch_pdl(k_or_gather, dim3(grid_for(n)), dim3(256), 0, (cudaStream_t)stream, dst, src, idx, n, invert);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -483,7 +515,7 @@ extern "C" int ph_batch_knn_kth(const float* pts, const ph_cloud_seg* segs, int3
   if (smem > 200 * 1024) return PH_ERR_ARG;
   if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_knn_batch);
   ph::count_launch();
-  k_knn_batch<<<(unsigned)nqb, KN_NT, smem, (cudaStream_t)stream>>>(pts, segs, nsegs, qb_off, k, out);
+  ph::launch_pdl(k_knn_batch, dim3((unsigned)nqb), dim3(KN_NT), smem, (cudaStream_t)stream, pts, segs, nsegs, qb_off, k, out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -504,11 +536,11 @@ extern "C" int ph_batch_quantile(const float* values, int64_t N, const int32_t* 
   if (!keys || !vals || !rws) return PH_ERR_ARG;
   if (N > 0) {
     ph::count_launch();
-    k_seg_value_keys<<<grid_for(N), 256, 0, s>>>(values, N, vcloud, keys, vals);
+    ph::launch_pdl(k_seg_value_keys, dim3(grid_for(N)), dim3(256), 0, s, values, N, vcloud, keys, vals);
     PH_TRY(radix_sort_pairs(keys, vals, N, 0, 64, rws, radix_sort_workspace_bytes(N), s));
   }
   ph::count_launch();
-  k_seg_quantile<<<grid_for(nsegs), 256, 0, s>>>(keys, segs, nsegs, (float)q, out);
+  ph::launch_pdl(k_seg_quantile, dim3(grid_for(nsegs)), dim3(256), 0, s, keys, segs, nsegs, (float)q, out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/flashph_b200.h"
 
 namespace ph {
@@ -47,6 +49,33 @@ int device_sms();
 // resident blocks per SM of func at this block size and dynamic shared
 // memory (cached; 0 when the query fails)
 int occupancy(const void* func, int threads, size_t smem);
+
+// Programmatic dependent launch. Kernels are launched with launch_pdl(), so
+// that the next kernel in the stream is scheduled while the current one
+// drains instead of after it (the launch latency between the ~80 short
+// kernels of a call is hidden). Every kernel starts with pdl_wait(), which
+// returns once the previous grid in the stream has completed and its memory
+// is visible (a no-op for a kernel not launched that way), and then lets its
+// own successor be scheduled with pdl_trigger(): the successor still waits in
+// its own pdl_wait() for this grid to complete.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 }  // namespace ph
 

@@ -57,6 +57,8 @@ __global__ void __launch_bounds__(ENT, 2)
     k_edges(const float* __restrict__ pts_all, const ph_cloud_seg* __restrict__ segs, int nsegs,
             ph_cloud_seg seg0, i32* __restrict__ oi, i32* __restrict__ oj, float* __restrict__ od,
             i64 cap, unsigned long long* __restrict__ count) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   __shared__ __align__(16) float xs[EK][ET];
   __shared__ __align__(16) float ys[EK][ET];
   const ph_cloud_seg sg = segs ? segs[find_seg(segs, nsegs, (i64)blockIdx.x)] : seg0;
@@ -148,6 +150,8 @@ __global__ void __launch_bounds__(ENT, 2)
 __global__ void k_edge_keys(const i32* __restrict__ ei, const i32* __restrict__ ej,
                             const float* __restrict__ dsq, i64 E, u64* __restrict__ keys,
                             u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     const u64 i = (u64)ei[e], j = (u64)ej[e];
     const u64 colex = j * (j - 1) / 2 + i;
@@ -167,6 +171,8 @@ __device__ __forceinline__ u64 emission_order(u64 i, u64 j, u64 nb32) {
 // stable argsort of its emitted edge list produces.
 __global__ void k_fix_ties(const u64* __restrict__ keys, u32* __restrict__ vals,
                            const i32* __restrict__ ei, const i32* __restrict__ ej, i64 E, u64 nb32) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < E; p += (i64)gridDim.x * blockDim.x) {
     const bool starts = (p == 0 || keys[p - 1] != keys[p]) && (p + 1 < E && keys[p + 1] == keys[p]);
     if (!starts) continue;
@@ -190,6 +196,8 @@ __global__ void k_fix_ties(const u64* __restrict__ keys, u32* __restrict__ vals,
 __global__ void k_gather_edges(const u32* __restrict__ perm, const i32* __restrict__ ei,
                                const i32* __restrict__ ej, const float* __restrict__ dsq, i64 E,
                                i32* __restrict__ oi, i32* __restrict__ oj, float* __restrict__ od) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     const u32 s = perm[e];
     oi[e] = ei[s];
@@ -202,6 +210,8 @@ __global__ void k_gather_edges(const u32* __restrict__ perm, const i32* __restri
 // half-edge keys (vertex << sh) | neighbour, sh = the bits of a vertex index
 __global__ void k_half_keys(const i32* __restrict__ ei, const i32* __restrict__ ej, i64 E, int sh,
                             u64* __restrict__ keys, u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
     const u64 i = (u64)(u32)ei[e], j = (u64)(u32)ej[e];
     keys[2 * e] = (i << sh) | j;
@@ -213,6 +223,8 @@ __global__ void k_half_keys(const i32* __restrict__ ei, const i32* __restrict__ 
 
 __global__ void k_csr_fill(const u64* __restrict__ keys, const u32* __restrict__ vals, i64 H, i64 n, int sh,
                            i32* __restrict__ ptr, i32* __restrict__ idx, i32* __restrict__ rank) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const u64 low = (1ull << sh) - 1;
   for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < H; p += (i64)gridDim.x * blockDim.x) {
     const u64 k = keys[p];
@@ -227,6 +239,8 @@ __global__ void k_csr_fill(const u64* __restrict__ keys, const u32* __restrict__
 }
 
 __global__ void k_sqrt(const float* __restrict__ in, float* __restrict__ out, i64 n) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
     out[i] = __fsqrt_rn(in[i]);
 }
@@ -254,7 +268,7 @@ extern "C" int ph_edges_enumerate(const float* pts, int64_t n, int32_t d, float 
     seg.d = d;
     seg.thr_sq = thr_sq;
     ph::count_launch();
-    k_edges<<<(unsigned)tiles, ENT, 0, s>>>(pts, nullptr, 1, seg, out_i, out_j, out_dsq, capacity, d_count);
+    ph::launch_pdl(k_edges, dim3((unsigned)tiles), dim3(ENT), 0, s, pts, nullptr, 1, seg, out_i, out_j, out_dsq, capacity, d_count);
   }
   PH_CHECK_LAUNCH();
   return PH_OK;
@@ -275,7 +289,7 @@ extern "C" int ph_batch_edges_enumerate(const float* pts, const ph_cloud_seg* se
   cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
   if (nsegs > 0 && ntiles > 0) {
     ph::count_launch();
-    k_edges<<<(unsigned)ntiles, ENT, 0, s>>>(pts, segs, nsegs, ph_cloud_seg{}, out_i, out_j, out_dsq, capacity,
+    ph::launch_pdl(k_edges, dim3((unsigned)ntiles), dim3(ENT), 0, s, pts, segs, nsegs, ph_cloud_seg{}, out_i, out_j, out_dsq, capacity,
                                              d_count);
   }
   PH_CHECK_LAUNCH();
@@ -298,14 +312,14 @@ extern "C" int ph_edges_sort(const int32_t* in_i, const int32_t* in_j, const flo
   void* rws = c.take<char>((i64)radix_sort_workspace_bytes(E));
   if (!keys || !vals || !rws) return PH_ERR_ARG;
   ph::count_launch();
-  k_edge_keys<<<grid_for(E), 256, 0, s>>>(in_i, in_j, in_dsq, E, keys, vals);
+  ph::launch_pdl(k_edge_keys, dim3(grid_for(E)), dim3(256), 0, s, in_i, in_j, in_dsq, E, keys, vals);
   PH_TRY(radix_sort_pairs(keys, vals, E, 0, 64, rws, radix_sort_workspace_bytes(E), s));
   if (n > 92682) {
     ph::count_launch();
-    k_fix_ties<<<grid_for(E), 256, 0, s>>>(keys, vals, in_i, in_j, E, (u64)((n + 31) / 32));
+    ph::launch_pdl(k_fix_ties, dim3(grid_for(E)), dim3(256), 0, s, keys, vals, in_i, in_j, E, (u64)((n + 31) / 32));
   }
   ph::count_launch();
-  k_gather_edges<<<grid_for(E), 256, 0, s>>>(vals, in_i, in_j, in_dsq, E, out_i, out_j, out_dsq);
+  ph::launch_pdl(k_gather_edges, dim3(grid_for(E)), dim3(256), 0, s, vals, in_i, in_j, in_dsq, E, out_i, out_j, out_dsq);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -334,10 +348,10 @@ extern "C" int ph_vertex_csr(const int32_t* edge_i, const int32_t* edge_j, int64
   while (sh < 32 && (int64_t(1) << sh) < n) ++sh;
   const int end_bit = std::min(64, ((2 * sh + 7) / 8) * 8);
   ph::count_launch();
-  k_half_keys<<<grid_for(E), 256, 0, s>>>(edge_i, edge_j, E, sh, keys, vals);
+  ph::launch_pdl(k_half_keys, dim3(grid_for(E)), dim3(256), 0, s, edge_i, edge_j, E, sh, keys, vals);
   PH_TRY(radix_sort_pairs(keys, vals, 2 * E, 0, end_bit, rws, radix_sort_workspace_bytes(2 * E), s));
   ph::count_launch();
-  k_csr_fill<<<grid_for(2 * E), 256, 0, s>>>(keys, vals, 2 * E, n, sh, adj_ptr, adj_idx, adj_rank);
+  ph::launch_pdl(k_csr_fill, dim3(grid_for(2 * E)), dim3(256), 0, s, keys, vals, 2 * E, n, sh, adj_ptr, adj_idx, adj_rank);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -346,7 +360,7 @@ extern "C" int ph_sqrt_f32(const float* in, float* out, int64_t count, void* str
   if (count < 0) return PH_ERR_ARG;
   if (count == 0) return PH_OK;
   ph::count_launch();
-  k_sqrt<<<grid_for(count), 256, 0, (cudaStream_t)stream>>>(in, out, count);
+  ph::launch_pdl(k_sqrt, dim3(grid_for(count)), dim3(256), 0, (cudaStream_t)stream, in, out, count);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

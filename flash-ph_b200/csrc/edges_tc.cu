@@ -186,6 +186,8 @@ struct ItemIt {
 
 // item_off[c] = items of clouds before c, item_off[nsegs] = total (one block)
 __global__ void k_tc_items(const ph_cloud_seg* __restrict__ segs, int nsegs, int nb, i64* __restrict__ item_off) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   __shared__ i64 part[1024];
   const int tid = threadIdx.x, nt = blockDim.x;
   const int chunk = (nsegs + nt - 1) / nt;
@@ -265,6 +267,8 @@ __device__ __forceinline__ void tma_load_2d(u32 dst, const CUtensorMap* map, int
 // sum of coordinates per cloud, FP64, from per-block partial sums (block = 128 points)
 __global__ void k_tc_mean(const float* __restrict__ pts, const ph_cloud_seg* __restrict__ segs, int nsegs,
                           const i64* __restrict__ blk_off, double* __restrict__ sum) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   __shared__ double part[TC_MAXK];
   const i64 b = blockIdx.x;
   const int c = find_off(blk_off, nsegs, b);
@@ -290,6 +294,8 @@ __global__ void k_tc_points(const float* __restrict__ pts, const ph_cloud_seg* _
                             const i64* __restrict__ blk_off, const double* __restrict__ sum, int kq, double kappa,
                             __nv_bfloat16* __restrict__ YA, __nv_bfloat16* __restrict__ YB,
                             float* __restrict__ blkrad) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   __shared__ float wmax[TC_T / 32];
   const i64 b = blockIdx.x;
   const int c = find_off(blk_off, nsegs, b);
@@ -485,6 +491,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                const i64* __restrict__ blk_off, const i64* __restrict__ item_off, const float* __restrict__ blkrad,
                TcShape sh, double thr_scale, i32* __restrict__ oi, i32* __restrict__ oj, float* __restrict__ od,
                i64 cap, unsigned long long* __restrict__ count, int* status, unsigned long long* __restrict__ stats) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long bars[BAR_N];
   __shared__ u32 tmem_sh;
@@ -898,16 +906,16 @@ extern "C" int ph_batch_edges_enumerate_screened(const float* pts, const ph_clou
   cudaMemsetAsync(sum, 0, sizeof(double) * nsegs * TC_MAXK, s);
   const double kappa = std::max(0x1p-11, (double)p.sh.kq * 0x1p-18);
   ph::count_launch();
-  k_tc_mean<<<(unsigned)nblocks, 256, 0, s>>>(pts, segs, nsegs, blk_off, sum);
+  ph::launch_pdl(k_tc_mean, dim3((unsigned)nblocks), dim3(256), 0, s, pts, segs, nsegs, blk_off, sum);
   ph::count_launch();
-  k_tc_points<<<(unsigned)nblocks, TC_T, 0, s>>>(pts, segs, nsegs, blk_off, sum, p.sh.kq, kappa, YA, YB, blkrad);
+  ph::launch_pdl(k_tc_points, dim3((unsigned)nblocks), dim3(TC_T), 0, s, pts, segs, nsegs, blk_off, sum, p.sh.kq, kappa, YA, YB, blkrad);
   ph::count_launch();
-  k_tc_items<<<1, 1024, 0, s>>>(segs, nsegs, p.sh.nb, item_off);
+  ph::launch_pdl(k_tc_items, dim3(1), dim3(1024), 0, s, segs, nsegs, p.sh.nb, item_off);
   const double thr_scale = 1.0 + (double)(max_d + 3) * 0x1p-24;
   // persistent: one CTA per SM, each a contiguous range of the items (counted on the device)
   const int grid = (int)std::min<i64>(ntiles, (i64)sms);
   ph::count_launch();
-  k_tc_edges<<<grid, TC_THREADS, p.smem, s>>>(tmA, tmB, pts, segs, nsegs, blk_off, item_off, blkrad, p.sh,
+  ph::launch_pdl(k_tc_edges, dim3(grid), dim3(TC_THREADS), p.smem, s, tmA, tmB, pts, segs, nsegs, blk_off, item_off, blkrad, p.sh,
                                               thr_scale, out_i, out_j, out_dsq, capacity, d_count, d_status, d_stats);
   PH_CHECK_LAUNCH();
   return PH_OK;

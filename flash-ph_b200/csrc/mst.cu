@@ -59,6 +59,8 @@ __device__ __forceinline__ i32 find_root(i32* parent, i32 v, int* status, MstCtl
 __global__ void __launch_bounds__(MST_NT) k_mst(const i32* __restrict__ ei, const i32* __restrict__ ej,
                                                i64 E, i64 n, i32* parent, i32* best, uint8_t* mst,
                                                i32* comp, MstCtl* ctl, int* status, int max_rounds) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   cg::grid_group g = cg::this_grid();
   const i64 tid = (i64)blockIdx.x * blockDim.x + threadIdx.x;
   const i64 nth = (i64)gridDim.x * blockDim.x;
@@ -179,6 +181,8 @@ __global__ void __launch_bounds__(MSTC_NT, 1) k_mst_cluster(const i32* __restric
                                                             i64 E, i64 n, i32* par_g, u64* offer, i32* minv,
                                                             uint8_t* __restrict__ mst, i32* __restrict__ comp,
                                                             MstCtl* ctl, int* status, int max_rounds) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   __shared__ int flag[2];  // rank 0's words: bit 0 some offer this round, bit 1 a loop bound was hit
   __shared__ int bad;
   cg::cluster_group cl = cg::this_cluster();
@@ -284,10 +288,14 @@ __global__ void __launch_bounds__(MSTC_NT, 1) k_mst_cluster(const i32* __restric
   cl.sync();  // rank 0's flag words stay valid until every block is done with them
 }
 
-__global__ void k_copy_ncomp(const MstCtl* ctl, int64_t* out) { *out = ctl->ncomp; }
+__global__ void k_copy_ncomp(const MstCtl* ctl, int64_t* out) {
+  ph::pdl_wait();
+  ph::pdl_trigger(); *out = ctl->ncomp; }
 
 __global__ void k_h0_rows(const float* __restrict__ filt, const uint8_t* __restrict__ mst,
                           const i32* __restrict__ pos, i64 E, i64 n, float* __restrict__ rows) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const i64 cnt = pos[E];
   for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x)
     if (mst[e]) {
@@ -380,7 +388,7 @@ extern "C" int ph_boruvka_mst(const int32_t* edge_i, const int32_t* edge_j, int6
       return PH_ERR_CUDA;
   } else if (work <= 4 * MST_NT * 8) {
     ph::count_launch();
-    k_mst<<<1, MST_NT, 0, s>>>(edge_i, edge_j, E, n, parent, best, mst_mask, comp, ctl, d_status, max_rounds);
+    ph::launch_pdl(k_mst, dim3(1), dim3(MST_NT), 0, s, edge_i, edge_j, E, n, parent, best, mst_mask, comp, ctl, d_status, max_rounds);
   } else {
     const int sms = ph::device_sms();
     const int per_sm = ph::occupancy((const void*)k_mst, MST_NT, 0);
@@ -395,7 +403,7 @@ extern "C" int ph_boruvka_mst(const int32_t* edge_i, const int32_t* edge_j, int6
       return PH_ERR_CUDA;
   }
   ph::count_launch();
-  k_copy_ncomp<<<1, 1, 0, s>>>(ctl, d_ncomp);
+  ph::launch_pdl(k_copy_ncomp, dim3(1), dim3(1), 0, s, ctl, d_ncomp);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -417,7 +425,7 @@ extern "C" int ph_h0_rows(const float* edge_filt, const uint8_t* mst_mask, int64
   const i64 work = std::max<i64>(E, n);
   const int g = (int)std::max<i64>(1, std::min<i64>((work + 255) / 256, 148 * 8));
   ph::count_launch();
-  k_h0_rows<<<g, 256, 0, s>>>(edge_filt, mst_mask, pos, E, n, out_rows);
+  ph::launch_pdl(k_h0_rows, dim3(g), dim3(256), 0, s, edge_filt, mst_mask, pos, E, n, out_rows);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -100,6 +100,8 @@ float to_f32(double v) {
 
 __global__ void k_single_seg(ph_cloud_seg* seg, int64_t* blk_off, int64_t n, int32_t d, float thr_sq,
                              int64_t nblocks) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   ph_cloud_seg s;
   s.pt_off = 0;
   s.vbase = 0;
@@ -233,7 +235,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   cudaMemsetAsync(cnt, 0, 8 * sizeof(int64_t), s);
   int* st = reinterpret_cast<int*>(cnt + 1);
   count_launch();
-  k_single_seg<<<1, 1, 0, s>>>(seg, blk, n, d, thr_sq, nblocks);
+  ph::launch_pdl(k_single_seg, dim3(1), dim3(1), 0, s, seg, blk, n, d, thr_sq, nblocks);
   const size_t ews = screened ? ph_edges_screened_workspace_bytes(n, 1, d) : 0;
   void* ew = screened ? A.bytes(ews) : nullptr;
   const i64 pairs = n * (n - 1) / 2;

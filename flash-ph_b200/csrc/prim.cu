@@ -47,6 +47,8 @@ __device__ __forceinline__ T block_excl_scan(T v, T* sm, T* total) {
 template <typename In, typename Out>
 __global__ void __launch_bounds__(SCAN_NT) k_scan_reduce(const In* __restrict__ in, i64 n,
                                                         Out* __restrict__ part, const int* active) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   if (active && !*active) return;
   __shared__ Out sm[SCAN_NT / 32];
   const i64 base = (i64)blockIdx.x * SCAN_TILE;
@@ -64,6 +66,8 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_reduce(const In* __restrict__ 
 template <typename Out>
 __global__ void __launch_bounds__(PART_NT) k_scan_partials(Out* __restrict__ part, i64 nparts,
                                                           Out* __restrict__ out_total, const int* active) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   if (active && !*active) return;
   __shared__ Out sm[PART_NT / 32];
   Out carry = 0;
@@ -82,6 +86,8 @@ template <typename In, typename Out>
 __global__ void __launch_bounds__(SCAN_NT) k_scan_down(const In* __restrict__ in, i64 n,
                                                       const Out* __restrict__ part,
                                                       Out* __restrict__ out, const int* active) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   if (active && !*active) return;
   __shared__ Out sm[SCAN_NT / 32];
   __shared__ Out tile[SCAN_TILE];
@@ -124,6 +130,8 @@ template <typename In, typename Out>
 __global__ void __launch_bounds__(SCAN_NT) k_scan_coop(const In* __restrict__ in, i64 n, i64 nparts,
                                                       Out* __restrict__ part, Out* __restrict__ out,
                                                       const int* active) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   if (active && !*active) return;  // the flag is the same for every block
   __shared__ Out sm[SCAN_NT / 32];
   __shared__ Out spre[COOP_MAX_PARTS];
@@ -211,11 +219,11 @@ int scan_impl(const In* in, Out* out, i64 n, void* ws, size_t ws_bytes, cudaStre
     }
   }
   ph::count_launch();
-  k_scan_reduce<In, Out><<<(unsigned)nparts, SCAN_NT, 0, s>>>(in, n, part, active);
+  ph::launch_pdl(k_scan_reduce<In, Out>, dim3((unsigned)nparts), dim3(SCAN_NT), 0, s, in, n, part, active);
   ph::count_launch();
-  k_scan_partials<Out><<<1, PART_NT, 0, s>>>(part, nparts, out + n, active);
+  ph::launch_pdl(k_scan_partials<Out>, dim3(1), dim3(PART_NT), 0, s, part, nparts, out + n, active);
   ph::count_launch();
-  k_scan_down<In, Out><<<(unsigned)nparts, SCAN_NT, 0, s>>>(in, n, part, out, active);
+  ph::launch_pdl(k_scan_down<In, Out>, dim3((unsigned)nparts), dim3(SCAN_NT), 0, s, in, n, part, out, active);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -252,6 +260,8 @@ struct SortCtl {
 
 __global__ void __launch_bounds__(RS_NT) k_os_hist(const u64* __restrict__ keys, i64 n, int p0, int p1,
                                                   SortCtl* ctl) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   __shared__ u32 h[8][256];
   for (int i = threadIdx.x; i < 8 * 256; i += RS_NT) h[i >> 8][i & 255] = 0;
   __syncthreads();
@@ -302,6 +312,8 @@ template <int RS_ROUNDS>
 __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u32* vB, i64 n, int p0,
                                                   int pass, SortCtl* ctl, unsigned long long* lb,
                                                   i64 ntiles) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   constexpr int RS_PER_WARP = 32 * RS_ROUNDS;
   constexpr int RS_TILE = rs_tile(RS_ROUNDS);
   __shared__ u32 tile_sh;
@@ -451,6 +463,8 @@ __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u3
 
 __global__ void k_os_finish(u64* __restrict__ kA, u32* __restrict__ vA, const u64* __restrict__ kB,
                             const u32* __restrict__ vB, i64 n, int p0, int p1, const SortCtl* ctl) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   u32 g[8];
 #pragma unroll
   for (int p = 0; p < 8; ++p) g[p] = (p >= p0 && p < p1) ? ctl->ghist[p][threadIdx.x] : 0u;
@@ -514,18 +528,18 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
   const int p0 = begin_bit / 8, p1 = end_bit / 8;
   const int gh = (int)std::max<i64>(1, std::min<i64>((n + RS_NT * 4 - 1) / (RS_NT * 4), 592));
   ph::count_launch();
-  k_os_hist<<<gh, RS_NT, 0, s>>>(keys, n, p0, p1, ctl);
+  ph::launch_pdl(k_os_hist, dim3(gh), dim3(RS_NT), 0, s, keys, n, p0, p1, ctl);
   const int gp = (int)std::min<i64>(ntiles, 148 * 4);
   for (int p = p0; p < p1; ++p) {
     ph::count_launch();
     if (rounds == RS_ROUNDS_SMALL)
-      k_os_pass<RS_ROUNDS_SMALL><<<gp, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
+      ph::launch_pdl(k_os_pass<RS_ROUNDS_SMALL>, dim3(gp), dim3(RS_NT), 0, s, keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
     else
-      k_os_pass<RS_ROUNDS_LARGE><<<gp, RS_NT, 0, s>>>(keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
+      ph::launch_pdl(k_os_pass<RS_ROUNDS_LARGE>, dim3(gp), dim3(RS_NT), 0, s, keys, vals, kB, vB, n, p0, p, ctl, lb, ntiles);
   }
   const int gf = (int)std::max<i64>(1, std::min<i64>((n + 255) / 256, 1184));
   ph::count_launch();
-  k_os_finish<<<gf, 256, 0, s>>>(keys, vals, kB, vB, n, p0, p1, ctl);
+  ph::launch_pdl(k_os_finish, dim3(gf), dim3(256), 0, s, keys, vals, kB, vB, n, p0, p1, ctl);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -85,6 +85,8 @@ __global__ void k_classify(const i32* __restrict__ off, const i32* __restrict__ 
                            i32 row_base, const uint8_t* __restrict__ skip, const i32* __restrict__ cmf,
                            i32* __restrict__ state, i32* __restrict__ piv, u64* __restrict__ owner,
                            u64* __restrict__ rec, i32* __restrict__ pool, i64 pool_cap, RedCtl* ctl, int* status) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const int lane = threadIdx.x & 31;
   const i64 stride = (i64)gridDim.x * blockDim.x;
   for (i64 c0 = (i64)blockIdx.x * blockDim.x + (threadIdx.x & ~31); c0 < K; c0 += stride) {
@@ -562,6 +564,8 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
                                                  const u64* __restrict__ rec, u64* owner, i32* pool, i64 pool_cap,
                                                  int chunk, RedCtl* ctl, int* status, int max_steps,
                                                  u32* dense_bits, i64 dense_words, int sm_words) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   extern __shared__ i32 rd_smem[];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   i32* const sW0 = rd_smem + (size_t)w * RD_WSTRIDE;  // working copies at sW0 and sW0 + RD_CAP
@@ -790,6 +794,8 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
 
 // residual columns default to empty (state 3) ...
 __global__ void k_finish_cols(i64 K, i32* __restrict__ state, i32* __restrict__ piv, const RedCtl* ctl, i64* info) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x) {
     if (state[c] != 2) continue;
     state[c] = 3;
@@ -806,6 +812,8 @@ __global__ void k_finish_cols(i64 K, i32* __restrict__ state, i32* __restrict__ 
 // ... and a residual column that owns a row at the end is paired with it
 __global__ void k_finish_rows(const u64* __restrict__ owner, i64 R, i32 row_base, i32* __restrict__ state,
                               i32* __restrict__ piv) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < R; r += (i64)gridDim.x * blockDim.x) {
     const u64 w = owner[r];
     if (!w) continue;
@@ -818,6 +826,8 @@ __global__ void k_finish_rows(const u64* __restrict__ owner, i64 R, i32 row_base
 
 __global__ void k_mark_pivots(const i32* __restrict__ state, const i32* __restrict__ piv, i64 K, i32 row_base,
                               uint8_t* __restrict__ flag) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x; c < K; c += (i64)gridDim.x * blockDim.x)
     if (state[c] == 1 || state[c] == 2) flag[piv[c] - row_base] = 1;
 }
@@ -884,7 +894,7 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   cudaMemsetAsync(owner, 0, sizeof(u64) * std::max<i64>(R, 1), s);
   cudaMemsetAsync(ctl, 0, sizeof(RedCtl), s);
   ph::count_launch();
-  k_classify<<<grid_for(K), 256, 0, s>>>(cof_off, cof_data, K, col_base, row_base, skip, row_cmf, col_state,
+  ph::launch_pdl(k_classify, dim3(grid_for(K)), dim3(256), 0, s, cof_off, cof_data, K, col_base, row_base, skip, row_cmf, col_state,
                                          col_piv, owner, rec, pool, pool_cap, ctl, d_status);
   if (ph::allow_dynamic_smem((const void*)k_reduce) != cudaSuccess) {
     PH_CHECK_LAUNCH();
@@ -897,13 +907,13 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   // pool chunk per warp: small enough that the chunks of all warps fit a quarter of the pool
   const int chunk = (int)std::max<i64>(64, std::min<i64>(2048, pool_cap / (4 * (i64)blocks * RD_WARPS)));
   ph::count_launch();
-  k_reduce<<<blocks, RD_NT, RD_SMEM, s>>>(row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
+  ph::launch_pdl(k_reduce, dim3(blocks), dim3(RD_NT), RD_SMEM, s, row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
                                           1 << 24, dense, dw, sm_dense_words(R));
   ph::count_launch();
-  k_finish_cols<<<grid_for(K), 256, 0, s>>>(K, col_state, col_piv, ctl, d_info);
+  ph::launch_pdl(k_finish_cols, dim3(grid_for(K)), dim3(256), 0, s, K, col_state, col_piv, ctl, d_info);
   if (R > 0) {
     ph::count_launch();
-    k_finish_rows<<<grid_for(R), 256, 0, s>>>(owner, R, row_base, col_state, col_piv);
+    ph::launch_pdl(k_finish_rows, dim3(grid_for(R)), dim3(256), 0, s, owner, R, row_base, col_state, col_piv);
   }
   PH_CHECK_LAUNCH();
   return PH_OK;
@@ -916,7 +926,7 @@ extern "C" int ph_mark_pivots(const int32_t* col_state, const int32_t* col_piv, 
   if (R > 0) cudaMemsetAsync(row_flag, 0, (size_t)R, s);
   if (K > 0) {
     ph::count_launch();
-    k_mark_pivots<<<grid_for(K), 256, 0, s>>>(col_state, col_piv, K, row_base, row_flag);
+    ph::launch_pdl(k_mark_pivots, dim3(grid_for(K)), dim3(256), 0, s, col_state, col_piv, K, row_base, row_flag);
   }
   PH_CHECK_LAUNCH();
   return PH_OK;

@@ -46,6 +46,8 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
                                                     const i64* __restrict__ tri_off, i32* __restrict__ tm,
                                                     i32* __restrict__ tw, i32* __restrict__ tfa,
                                                     i32* __restrict__ tfb) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
@@ -102,6 +104,8 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
 __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ aptr, const i32* __restrict__ aidx,
                                                     i64 n, int* __restrict__ next,
                                                     unsigned long long* __restrict__ total) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   extern __shared__ u32 nbits[];
   __shared__ int cur;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -151,6 +155,8 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
                                                const i32* __restrict__ arank, const uint8_t* __restrict__ enable,
                                                i32* __restrict__ tet_cnt, const i64* __restrict__ tet_off,
                                                i32* __restrict__ qm, i32* __restrict__ qf, int* status) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const int lane = threadIdx.x & 31;
   const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
@@ -220,6 +226,8 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
 __global__ void k_cof_entries(const i32* __restrict__ faos, const i32* __restrict__ f0,
                               const i32* __restrict__ f1, const i32* __restrict__ f2, int k, i64 S,
                               i32 row_base, u64* __restrict__ keys, u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const i64 total = S * k;
   for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (i64)gridDim.x * blockDim.x) {
     const i64 s = x / k;
@@ -234,6 +242,8 @@ __global__ void k_cof_entries(const i32* __restrict__ faos, const i32* __restric
 
 __global__ void k_cof_fill(const u64* __restrict__ keys, const u32* __restrict__ vals, i64 H, i64 nf,
                            i32* __restrict__ off, i32* __restrict__ data) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x; p < H; p += (i64)gridDim.x * blockDim.x) {
     const i64 f = (i64)keys[p];
     data[p] = (i32)vals[p];
@@ -247,6 +257,8 @@ __global__ void k_cof_fill(const u64* __restrict__ keys, const u32* __restrict__
 __global__ void k_cmf(const i32* __restrict__ faos, const i32* __restrict__ f0, const i32* __restrict__ f1,
                       const i32* __restrict__ f2, int k, i64 S, i32 face_base,
                       const uint8_t* __restrict__ skip, i32* __restrict__ cmf) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 s = (i64)blockIdx.x * blockDim.x + threadIdx.x; s < S; s += (i64)gridDim.x * blockDim.x) {
     i32 best = -1;
     for (int z = 0; z < k; ++z) {
@@ -288,7 +300,7 @@ extern "C" int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, 
   if (!tc || !cc || !sws) return PH_ERR_ARG;
   if (E > 0) {
     ph::count_launch();
-    k_triangles<false><<<warp_grid(E), SX_NT, 0, s>>>(edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, tc, cc,
+    ph::launch_pdl(k_triangles<false>, dim3(warp_grid(E)), dim3(SX_NT), 0, s, edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, tc, cc,
                                                       nullptr, nullptr, nullptr, nullptr, nullptr);
   }
   PH_TRY(scan_exclusive_i32_i64(tc, tri_off, E, sws, scan_workspace_bytes(E), s));
@@ -322,7 +334,7 @@ extern "C" int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx
   const int occ = ph::occupancy((const void*)k_tri_total, SX_NT, smem);
   const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
   ph::count_launch();
-  k_tri_total<<<grid, SX_NT, smem, s>>>(adj_ptr, adj_idx, n, d_next, d_total);
+  ph::launch_pdl(k_tri_total, dim3(grid), dim3(SX_NT), smem, s, adj_ptr, adj_idx, n, d_next, d_total);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -333,7 +345,7 @@ extern "C" int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, i
                                  int32_t* tri_fb, void* stream) {
   if (E <= 0) return E < 0 ? PH_ERR_ARG : PH_OK;
   ph::count_launch();
-  k_triangles<true><<<warp_grid(E), SX_NT, 0, (cudaStream_t)stream>>>(
+  ph::launch_pdl(k_triangles<true>, dim3(warp_grid(E)), dim3(SX_NT), 0, (cudaStream_t)stream, 
       edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, nullptr, nullptr, tri_off, tri_m, tri_w, tri_fa, tri_fb);
   PH_CHECK_LAUNCH();
   return PH_OK;
@@ -355,7 +367,7 @@ extern "C" int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64
   if (!qc || !sws) return PH_ERR_ARG;
   if (E > 0) {
     ph::count_launch();
-    k_tets<false><<<warp_grid(E), SX_NT, 0, s>>>(nullptr, nullptr, E, tri_off, tri_w, nullptr, nullptr, adj_ptr,
+    ph::launch_pdl(k_tets<false>, dim3(warp_grid(E)), dim3(SX_NT), 0, s, nullptr, nullptr, E, tri_off, tri_w, nullptr, nullptr, adj_ptr,
                                                  adj_idx, adj_rank, edge_enable, qc, nullptr, nullptr, nullptr,
                                                  nullptr);
   }
@@ -371,7 +383,7 @@ extern "C" int ph_tets_emit(const int32_t* edge_i, const int32_t* edge_j, int64_
                             int32_t* tet_faces, int* d_status, void* stream) {
   if (E <= 0) return E < 0 ? PH_ERR_ARG : PH_OK;
   ph::count_launch();
-  k_tets<true><<<warp_grid(E), SX_NT, 0, (cudaStream_t)stream>>>(edge_i, edge_j, E, tri_off, tri_w, tri_fa,
+  ph::launch_pdl(k_tets<true>, dim3(warp_grid(E)), dim3(SX_NT), 0, (cudaStream_t)stream, edge_i, edge_j, E, tri_off, tri_w, tri_fa,
                                                                 tri_fb, adj_ptr, adj_idx, adj_rank, edge_enable,
                                                                 nullptr, tet_off, tet_m, tet_faces, d_status);
   PH_CHECK_LAUNCH();
@@ -403,14 +415,14 @@ extern "C" int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const
   void* rws = c.take<char>((i64)radix_sort_workspace_bytes(H));
   if (!keys || !vals || !rws) return PH_ERR_ARG;
   ph::count_launch();
-  k_cof_entries<<<grid_for(H), 256, 0, s>>>(faces_aos, f0, f1, f2, k, S, row_base, keys, vals);
+  ph::launch_pdl(k_cof_entries, dim3(grid_for(H)), dim3(256), 0, s, faces_aos, f0, f1, f2, k, S, row_base, keys, vals);
   // face indices are below n_faces: sort only the bytes they use (stable, so
   // the simplices of a face stay in ascending order)
   int fb = 1;
   while (fb < 32 && (int64_t(1) << fb) < n_faces) ++fb;
   PH_TRY(radix_sort_pairs(keys, vals, H, 0, std::min(32, ((fb + 7) / 8) * 8), rws, radix_sort_workspace_bytes(H), s));
   ph::count_launch();
-  k_cof_fill<<<grid_for(H), 256, 0, s>>>(keys, vals, H, n_faces, cof_off, cof_data);
+  ph::launch_pdl(k_cof_fill, dim3(grid_for(H)), dim3(256), 0, s, keys, vals, H, n_faces, cof_off, cof_data);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -421,7 +433,7 @@ extern "C" int ph_cof_max_face(const int32_t* faces_aos, const int32_t* f0, cons
   if (k < 1 || k > 4 || S < 0) return PH_ERR_ARG;
   if (S == 0) return PH_OK;
   ph::count_launch();
-  k_cmf<<<grid_for(S), 256, 0, (cudaStream_t)stream>>>(faces_aos, f0, f1, f2, k, S, face_base, skip, cmf);
+  ph::launch_pdl(k_cmf, dim3(grid_for(S)), dim3(256), 0, (cudaStream_t)stream, faces_aos, f0, f1, f2, k, S, face_base, skip, cmf);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -22,6 +22,8 @@ constexpr int KN_MAXK = 64;
 
 __global__ void __launch_bounds__(KN_NT) k_knn(const float* __restrict__ pts, i64 n, int d, int k,
                                               float* __restrict__ out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   extern __shared__ float sm[];
   float* q = sm;                 // [d][KN_NT]
   float* tile = sm + d * KN_NT;  // [KN_TP][d]
@@ -61,6 +63,8 @@ __global__ void __launch_bounds__(KN_NT) k_knn(const float* __restrict__ pts, i6
 
 __global__ void __launch_bounds__(KN_NT) k_enclosing(const float* __restrict__ pts, i64 n, int d,
                                                     unsigned int* __restrict__ best_bits) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   extern __shared__ float sm[];
   float* q = sm;
   float* tile = sm + d * KN_NT;
@@ -92,6 +96,8 @@ __global__ void __launch_bounds__(KN_NT) k_enclosing(const float* __restrict__ p
 // torch.quantile (linear): rank = q * (n - 1) in float32, lerp between the
 // neighbouring order statistics with torch's two-sided lerp formula.
 __global__ void k_quantile(const u64* __restrict__ sorted_bits, i64 n, float qf, float* out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   const float rank = __fmul_rn(qf, (float)(n - 1));
   i64 lo = (i64)rank;
   const float w = __fsub_rn(rank, (float)lo);
@@ -107,6 +113,8 @@ __global__ void k_quantile(const u64* __restrict__ sorted_bits, i64 n, float qf,
 }
 
 __global__ void k_float_keys(const float* __restrict__ v, i64 n, u64* __restrict__ keys, u32* __restrict__ vals) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
     u32 b = __float_as_uint(v[i]);
     b = (b & 0x80000000u) ? ~b : (b | 0x80000000u);  // order-preserving for all floats
@@ -116,6 +124,8 @@ __global__ void k_float_keys(const float* __restrict__ v, i64 n, u64* __restrict
 }
 
 __global__ void k_unflip(u64* __restrict__ keys, i64 n) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
     u32 b = (u32)(keys[i] >> 32);
     b = (b & 0x80000000u) ? (b & 0x7fffffffu) : ~b;
@@ -123,7 +133,9 @@ __global__ void k_unflip(u64* __restrict__ keys, i64 n) {
   }
 }
 
-__global__ void k_bits_to_float(const unsigned int* bits, float* out) { *out = __uint_as_float(*bits); }
+__global__ void k_bits_to_float(const unsigned int* bits, float* out) {
+  ph::pdl_wait();
+  ph::pdl_trigger(); *out = __uint_as_float(*bits); }
 
 inline int grid_for(i64 n, int nt = 256) {
   return (int)std::max<i64>(1, std::min<i64>((n + nt - 1) / nt, 148 * 16));
@@ -142,7 +154,7 @@ extern "C" int ph_knn_kth(const float* pts, int64_t n, int32_t d, int32_t k, flo
   if (smem > 200 * 1024) return PH_ERR_ARG;
   if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_knn);
   ph::count_launch();
-  k_knn<<<(unsigned)((n + KN_NT - 1) / KN_NT), KN_NT, smem, (cudaStream_t)stream>>>(pts, n, d, k, out);
+  ph::launch_pdl(k_knn, dim3((unsigned)((n + KN_NT - 1) / KN_NT)), dim3(KN_NT), smem, (cudaStream_t)stream, pts, n, d, k, out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -161,12 +173,12 @@ extern "C" int ph_quantile_f32(const float* values, int64_t n, double q, float* 
   void* rws = c.take<char>((i64)radix_sort_workspace_bytes(n));
   if (!keys || !vals || !rws) return PH_ERR_ARG;
   ph::count_launch();
-  k_float_keys<<<grid_for(n), 256, 0, s>>>(values, n, keys, vals);
+  ph::launch_pdl(k_float_keys, dim3(grid_for(n)), dim3(256), 0, s, values, n, keys, vals);
   PH_TRY(radix_sort_pairs(keys, vals, n, 32, 64, rws, radix_sort_workspace_bytes(n), s));
   ph::count_launch();
-  k_unflip<<<grid_for(n), 256, 0, s>>>(keys, n);
+  ph::launch_pdl(k_unflip, dim3(grid_for(n)), dim3(256), 0, s, keys, n);
   ph::count_launch();
-  k_quantile<<<1, 1, 0, s>>>(keys, n, (float)q, d_out);
+  ph::launch_pdl(k_quantile, dim3(1), dim3(1), 0, s, keys, n, (float)q, d_out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -188,9 +200,9 @@ extern "C" int ph_enclosing_radius(const float* pts, int64_t n, int32_t d, float
   if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_enclosing);
   cudaMemsetAsync(bits, 0x7f, sizeof(unsigned int), s);
   ph::count_launch();
-  k_enclosing<<<(unsigned)((n + KN_NT - 1) / KN_NT), KN_NT, smem, s>>>(pts, n, d, bits);
+  ph::launch_pdl(k_enclosing, dim3((unsigned)((n + KN_NT - 1) / KN_NT)), dim3(KN_NT), smem, s, pts, n, d, bits);
   ph::count_launch();
-  k_bits_to_float<<<1, 1, 0, s>>>(bits, d_out);
+  ph::launch_pdl(k_bits_to_float, dim3(1), dim3(1), 0, s, bits, d_out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
