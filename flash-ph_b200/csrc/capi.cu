@@ -1,4 +1,5 @@
 // Library-wide C entry points: version, error reporting, launch counting.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -55,6 +56,36 @@ cudaError_t allow_dynamic_smem(const void* func) {
     e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
   if (e == cudaSuccess) g_smem_set.push_back({dev, func, 0, 0, 1});
   return e;
+}
+
+namespace {
+// zeroes one or two byte ranges: 16-byte stores where a range is aligned, bytes
+// for its unaligned head and tail
+__device__ void zero_range(uint8_t* p, size_t n) {
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (size_t)gridDim.x * blockDim.x;
+  const size_t head = std::min<size_t>(n, (16 - (reinterpret_cast<uintptr_t>(p) & 15)) & 15);
+  for (size_t i = tid; i < head; i += nth) p[i] = 0;
+  const size_t body = (n - head) / 16;
+  uint4* q = reinterpret_cast<uint4*>(p + head);
+  for (size_t i = tid; i < body; i += nth) q[i] = make_uint4(0, 0, 0, 0);
+  for (size_t i = head + body * 16 + tid; i < n; i += nth) p[i] = 0;
+}
+__global__ void k_zero(uint8_t* p1, size_t n1, uint8_t* p2, size_t n2) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  if (p1) zero_range(p1, n1);
+  if (p2) zero_range(p2, n2);
+}
+}  // namespace
+
+cudaError_t zero_async(void* p1, size_t n1, cudaStream_t s, void* p2, size_t n2) {
+  if (!p1) n1 = 0;
+  if (!p2) n2 = 0;
+  const size_t most = std::max(n1, n2);
+  if (most == 0) return cudaSuccess;
+  const int grid = (int)std::min<size_t>((most + 256 * 16 - 1) / (256 * 16), 296);
+  count_launch();
+  return launch_pdl(k_zero, dim3(grid), dim3(256), 0, s, static_cast<uint8_t*>(p1), n1, static_cast<uint8_t*>(p2), n2);
 }
 
 int occupancy(const void* func, int threads, size_t smem) {

@@ -44,6 +44,9 @@ void count_launch();
 // so threads launching the kernel concurrently with different requests
 // cannot lower each other's limit. Returns cudaSuccess or the error.
 cudaError_t allow_dynamic_smem(const void* func);
+// Zeroes n1 bytes at p1 (and n2 bytes at p2) with one kernel launched like
+// every other (a memset node would end the chain of dependent launches).
+cudaError_t zero_async(void* p1, size_t n1, cudaStream_t s, void* p2 = nullptr, size_t n2 = 0);
 // SM count of the current device (cached)
 int device_sms();
 // resident blocks per SM of func at this block size and dynamic shared

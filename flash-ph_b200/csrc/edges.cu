@@ -258,7 +258,7 @@ extern "C" int ph_edges_enumerate(const float* pts, int64_t n, int32_t d, float 
   cudaStream_t s = (cudaStream_t)stream;
   if (n < 0 || d <= 0 || capacity < 0 || !d_count) return PH_ERR_ARG;
   if (n >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
-  cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  ph::zero_async(d_count, sizeof(unsigned long long), s);
   if (n >= 2) {
     const i64 nt = (n + ET - 1) / ET;
     const i64 tiles = nt * (nt + 1) / 2;
@@ -286,7 +286,7 @@ extern "C" int ph_batch_edges_enumerate(const float* pts, const ph_cloud_seg* se
   cudaStream_t s = (cudaStream_t)stream;
   if (nsegs < 0 || ntiles < 0 || capacity < 0 || !d_count) return PH_ERR_ARG;
   if (ntiles >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
-  cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  ph::zero_async(d_count, sizeof(unsigned long long), s);
   if (nsegs > 0 && ntiles > 0) {
     ph::count_launch();
     ph::launch_pdl(k_edges, dim3((unsigned)ntiles), dim3(ENT), 0, s, pts, segs, nsegs, ph_cloud_seg{}, out_i, out_j, out_dsq, capacity,
@@ -334,7 +334,7 @@ extern "C" int ph_vertex_csr(const int32_t* edge_i, const int32_t* edge_j, int64
   cudaStream_t s = (cudaStream_t)stream;
   if (E < 0 || 2 * E >= (int64_t(1) << 31) || n < 0) return PH_ERR_OVERFLOW;
   if (E == 0) {
-    cudaMemsetAsync(adj_ptr, 0, sizeof(int32_t) * (n + 1), s);
+    ph::zero_async(adj_ptr, sizeof(int32_t) * (n + 1), s);
     PH_CHECK_LAUNCH();
     return PH_OK;
   }

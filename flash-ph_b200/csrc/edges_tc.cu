@@ -883,8 +883,8 @@ extern "C" int ph_batch_edges_enumerate_screened(const float* pts, const ph_clou
     record_message("ph_batch_edges_enumerate_screened: workspace too small");
     return PH_ERR_ARG;
   }
-  cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
   if (ntiles == 0 || N == 0 || nblocks == 0) {
+    ph::zero_async(d_count, sizeof(unsigned long long), s);
     PH_CHECK_LAUNCH();
     return PH_OK;
   }
@@ -903,7 +903,7 @@ extern "C" int ph_batch_edges_enumerate_screened(const float* pts, const ph_clou
     record_message("ph_batch_edges_enumerate_screened: expected one CTA per SM for the TMEM budget");
     return PH_ERR_CUDA;
   }
-  cudaMemsetAsync(sum, 0, sizeof(double) * nsegs * TC_MAXK, s);
+  ph::zero_async(sum, sizeof(double) * nsegs * TC_MAXK, s, d_count, sizeof(unsigned long long));
   const double kappa = std::max(0x1p-11, (double)p.sh.kq * 0x1p-18);
   ph::count_launch();
   ph::launch_pdl(k_tc_mean, dim3((unsigned)nblocks), dim3(256), 0, s, pts, segs, nsegs, blk_off, sum);

@@ -354,7 +354,7 @@ extern "C" int ph_boruvka_mst(const int32_t* edge_i, const int32_t* edge_j, int6
   cudaStream_t s = (cudaStream_t)stream;
   if (n < 0 || E < 0 || n >= (int64_t(1) << 31) || E >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
   if (n == 0) {
-    cudaMemsetAsync(d_ncomp, 0, sizeof(int64_t), s);
+    ph::zero_async(d_ncomp, sizeof(int64_t), s);
     PH_CHECK_LAUNCH();
     return PH_OK;
   }

@@ -98,10 +98,12 @@ float to_f32(double v) {
   return (float)v;
 }
 
+// the segment record of a single cloud, and the run's counters cleared
 __global__ void k_single_seg(ph_cloud_seg* seg, int64_t* blk_off, int64_t n, int32_t d, float thr_sq,
-                             int64_t nblocks) {
+                             int64_t nblocks, int64_t* cnt) {
   ph::pdl_wait();
   ph::pdl_trigger();
+  for (int k = 0; k < 8; ++k) cnt[k] = 0;
   ph_cloud_seg s;
   s.pt_off = 0;
   s.vbase = 0;
@@ -232,10 +234,9 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   // cnt[5] triangle total, cnt[6] its work counter
   int64_t* cnt = A.take<int64_t>(8);
   if (A.failed) return alloc_fail();
-  cudaMemsetAsync(cnt, 0, 8 * sizeof(int64_t), s);
   int* st = reinterpret_cast<int*>(cnt + 1);
   count_launch();
-  ph::launch_pdl(k_single_seg, dim3(1), dim3(1), 0, s, seg, blk, n, d, thr_sq, nblocks);
+  ph::launch_pdl(k_single_seg, dim3(1), dim3(1), 0, s, seg, blk, n, d, thr_sq, nblocks, cnt);
   const size_t ews = screened ? ph_edges_screened_workspace_bytes(n, 1, d) : 0;
   void* ew = screened ? A.bytes(ews) : nullptr;
   const i64 pairs = n * (n - 1) / 2;
@@ -290,7 +291,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (rc == PH_OK) rc = ph_sqrt_f32(sd, filt, E, s);
     if (rc != PH_OK) return give_up(rc);
   } else {
-    cudaMemsetAsync(adj_ptr, 0, sizeof(i32) * (n + 1), s);
+    ph::zero_async(adj_ptr, sizeof(i32) * (n + 1), s);
   }
 
   // ---- 3. H0 (boruvka.py, persistence.py:169-192) ---------------------------------------------
@@ -378,7 +379,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (rc == PH_OK) rc = ph_cof_max_face(nullptr, tri_m, tri_fa, tri_fb, 3, T, 0, mask, cmf1, s);
     if (rc != PH_OK) return give_up(rc);
   } else {
-    cudaMemsetAsync(off1, 0, sizeof(i32) * (E + 1), s);
+    ph::zero_async(off1, sizeof(i32) * (E + 1), s);
   }
 
   // ---- 5. H1 reduction and rows (reduce_h1_gpu.py:159-223, 574-604) --------------------------
@@ -409,7 +410,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
       return give_up(fail(st_red, "ph_reduce (H1) failed"));
     pool1 = std::min<i64>(pool1 * 4, POOL_MAX);
-    cudaMemsetAsync(st + 2, 0, sizeof(int), s);
+    ph::zero_async(st + 2, sizeof(int), s);
   }
   res->nrows[1] = H[1];
   res->stats[3] = H[2];
@@ -454,7 +455,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (rc == PH_OK && Q)
       rc = ph_cofacet_csr(tet_faces, nullptr, nullptr, nullptr, 4, Q, T, (i32)(E + T), off2, data2, c2_ws, c2_b, s);
     if (rc != PH_OK) return give_up(rc);
-    if (!Q) cudaMemsetAsync(off2, 0, sizeof(i32) * (T + 1), s);
+    if (!Q) ph::zero_async(off2, sizeof(i32) * (T + 1), s);
   }
   i64 pool2 = pool_capacity(4 * Q, T);
   RedOut r2{};
@@ -470,7 +471,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool2 >= POOL_MAX)
       return give_up(fail(st_red, "ph_reduce (H2) failed"));
     pool2 = std::min<i64>(pool2 * 4, POOL_MAX);
-    cudaMemsetAsync(st + 4, 0, sizeof(int), s);
+    ph::zero_async(st + 4, sizeof(int), s);
   }
   res->nrows[2] = H[2];
   res->stats[4] = H[3];

@@ -198,7 +198,7 @@ int scan_impl(const In* in, Out* out, i64 n, void* ws, size_t ws_bytes, cudaStre
               const int* active) {
   if (n < 0) return PH_ERR_ARG;
   if (n == 0) {
-    cudaMemsetAsync(out, 0, sizeof(Out), s);
+    ph::zero_async(out, sizeof(Out), s);
     PH_CHECK_LAUNCH();
     return PH_OK;
   }
@@ -524,7 +524,7 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
   if (!kB || !vB || !ctl || !lb) return PH_ERR_ARG;
   // ctl and lb are adjacent in the workspace: one memset clears both
   const size_t clear = (size_t)((char*)(lb + ntiles * 256) - (char*)ctl);
-  cudaMemsetAsync(ctl, 0, clear, s);
+  ph::zero_async(ctl, clear, s);
   const int p0 = begin_bit / 8, p1 = end_bit / 8;
   const int gh = (int)std::max<i64>(1, std::min<i64>((n + RS_NT * 4 - 1) / (RS_NT * 4), 592));
   ph::count_launch();

@@ -882,7 +882,7 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   if (K >= (int64_t(1) << 31) || R >= (int64_t(1) << 31) || pool_cap >= (int64_t(1) << OW_SHIFT))
     return PH_ERR_OVERFLOW;
   if (K == 0) {
-    if (d_info) cudaMemsetAsync(d_info, 0, 4 * sizeof(int64_t), s);
+    if (d_info) ph::zero_async(d_info, 4 * sizeof(int64_t), s);
     PH_CHECK_LAUNCH();
     return PH_OK;
   }
@@ -891,8 +891,7 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   u64* rec = c.take<u64>(K);
   RedCtl* ctl = c.take<RedCtl>(1);
   if (!owner || !rec || !ctl) return PH_ERR_ARG;
-  cudaMemsetAsync(owner, 0, sizeof(u64) * std::max<i64>(R, 1), s);
-  cudaMemsetAsync(ctl, 0, sizeof(RedCtl), s);
+  ph::zero_async(owner, sizeof(u64) * std::max<i64>(R, 1), s, ctl, sizeof(RedCtl));
   ph::count_launch();
   ph::launch_pdl(k_classify, dim3(grid_for(K)), dim3(256), 0, s, cof_off, cof_data, K, col_base, row_base, skip, row_cmf, col_state,
                                          col_piv, owner, rec, pool, pool_cap, ctl, d_status);
@@ -923,7 +922,7 @@ extern "C" int ph_mark_pivots(const int32_t* col_state, const int32_t* col_piv, 
                               uint8_t* row_flag, int64_t R, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (K < 0 || R < 0) return PH_ERR_ARG;
-  if (R > 0) cudaMemsetAsync(row_flag, 0, (size_t)R, s);
+  if (R > 0) ph::zero_async(row_flag, (size_t)R, s);
   if (K > 0) {
     ph::count_launch();
     ph::launch_pdl(k_mark_pivots, dim3(grid_for(K)), dim3(256), 0, s, col_state, col_piv, K, row_base, row_flag);

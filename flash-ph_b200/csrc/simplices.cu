@@ -319,8 +319,7 @@ extern "C" int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx
     record_message("ph_triangles_total: n exceeds the shared-memory bitmap (1638400 vertices)");
     return PH_ERR_ARG;
   }
-  cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s);
-  cudaMemsetAsync(d_next, 0, sizeof(int), s);
+  ph::zero_async(d_total, sizeof(unsigned long long), s, d_next, sizeof(int));
   if (n < 3) {
     PH_CHECK_LAUNCH();
     return PH_OK;
@@ -405,7 +404,7 @@ extern "C" int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const
   const i64 H = S * k;
   if (H >= (int64_t(1) << 31) || (i64)row_base + S >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
   if (H == 0) {
-    cudaMemsetAsync(cof_off, 0, sizeof(int32_t) * (n_faces + 1), s);
+    ph::zero_async(cof_off, sizeof(int32_t) * (n_faces + 1), s);
     PH_CHECK_LAUNCH();
     return PH_OK;
   }
