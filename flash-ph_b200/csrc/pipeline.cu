@@ -65,15 +65,36 @@ struct Arena {
   }
 };
 
-// small pinned host buffer per thread for count and status readbacks
-int64_t* pinned_slots() {
-  thread_local int64_t* buf = nullptr;
-  if (!buf) {
+// small pinned, device-mapped host buffer per thread for count and status
+// readbacks (a kernel writes the values into it directly)
+struct Slots {
+  int64_t* host = nullptr;
+  int64_t* dev = nullptr;
+};
+Slots pinned_slots() {
+  thread_local Slots b;
+  if (!b.host) {
     void* p = nullptr;
-    if (cudaMallocHost(&p, 64 * sizeof(int64_t)) != cudaSuccess) return nullptr;
-    buf = static_cast<int64_t*>(p);
+    if (cudaHostAlloc(&p, 64 * sizeof(int64_t), cudaHostAllocMapped) != cudaSuccess) return Slots{};
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
+      cudaFreeHost(p);
+      return Slots{};
+    }
+    b.host = static_cast<int64_t*>(p);
+    b.dev = static_cast<int64_t*>(d);
   }
-  return buf;
+  return b;
+}
+
+// copies up to four device int64 values into the mapped host slots
+__global__ void k_report(const int64_t* a, const int64_t* b, const int64_t* c, const int64_t* d, int count,
+                         volatile int64_t* out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  const int64_t* src[4] = {a, b, c, d};
+  if (threadIdx.x < count && threadIdx.x < 4) out[threadIdx.x] = *src[threadIdx.x];
+  __threadfence_system();
 }
 
 // keeps the device's stream-ordered pool from returning memory at every sync
@@ -129,15 +150,17 @@ cudaEvent_t wait_event() {
   return ev;
 }
 
-// copies count int64 values (device) to the pinned slots and waits: polls
-// for up to half a millisecond (the usual wait is a few microseconds, and a
-// blocking wait adds its wake-up latency to every readback), then blocks
-int readback(const int64_t* const* src, int count, int64_t* dst, cudaStream_t s) {
-  for (int k = 0; k < count; ++k)
-    if (cudaMemcpyAsync(dst + k, src[k], sizeof(int64_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
-      record_error(cudaGetLastError());
-      return PH_ERR_CUDA;
-    }
+// brings count (<= 4) int64 values from the device into the pinned slots (one
+// kernel writes them into the mapped host buffer) and waits: polls for up to
+// half a millisecond (the usual wait is a few microseconds, and a blocking
+// wait adds its wake-up latency to every readback), then blocks
+int readback(const int64_t* const* src, int count, const Slots& dst, cudaStream_t s) {
+  count_launch();
+  if (ph::launch_pdl(k_report, dim3(1), dim3(32), 0, s, src[0], count > 1 ? src[1] : src[0],
+                     count > 2 ? src[2] : src[0], count > 3 ? src[3] : src[0], count, dst.dev) != cudaSuccess) {
+    record_error(cudaGetLastError());
+    return PH_ERR_CUDA;
+  }
   cudaEvent_t ev = wait_event();
   if (ev && cudaEventRecord(ev, s) == cudaSuccess) {
     const auto t0 = std::chrono::steady_clock::now();
@@ -207,8 +230,9 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   int dev = 0;
   cudaGetDevice(&dev);
   keep_pool(dev);
-  int64_t* H = pinned_slots();
-  if (!H) return fail(PH_ERR_CUDA, "ph_rips_persistence: pinned host buffer unavailable");
+  const Slots slots = pinned_slots();
+  if (!slots.host) return fail(PH_ERR_CUDA, "ph_rips_persistence: pinned host buffer unavailable");
+  volatile int64_t* H = slots.host;
 
   Arena A(s);
   ph_result* res = new ph_result();
@@ -259,7 +283,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
                                     reinterpret_cast<unsigned long long*>(cnt), s);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[2] = {cnt, cnt + 1};
-    if (readback(src, 2, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    if (readback(src, 2, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_e = (int)(H[1] & 0xffffffff);
     if (st_e) return give_up(fail(st_e, "edge enumeration failed"));
     E = H[0];
@@ -311,7 +335,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   res->nrows[0] = n;
   if (max_dim == 0) {
     const int64_t* src[1] = {cnt + 1};
-    if (readback(src, 1, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    if (readback(src, 1, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_mst = (int)(H[0] >> 32);
     if (st_mst) return give_up(fail(st_mst, "ph_boruvka_mst failed"));
     A.release_to(res);
@@ -335,12 +359,12 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
                                 reinterpret_cast<int*>(cnt + 6), s);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[2] = {cnt + 5, cnt + 1};
-    if (readback(src, 2, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    if (readback(src, 2, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
   } else {
     int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[2] = {tri_off + E, cnt + 1};
-    if (readback(src, 2, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    if (readback(src, 2, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
   }
   const i64 T = H[0];
   if ((int)(H[1] >> 32) != 0) return give_up(fail((int)(H[1] >> 32), "ph_boruvka_mst failed"));
@@ -404,7 +428,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
       if (rc != PH_OK) return give_up(rc);
     }
     const int64_t* src[4] = {cnt + 2, r1.nrows, r1.info + 1, max_dim == 2 ? tet_off + E : r1.nrows};
-    if (readback(src, 4, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    if (readback(src, 4, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_red = (int)(H[0] & 0xffffffff);
     if (st_red == PH_OK) break;
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
@@ -464,7 +488,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
                          st + 4, res->rows[2], r2);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[4] = {cnt + 2, cnt + 3, r2.nrows, r2.info + 1};
-    if (readback(src, 4, H, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    if (readback(src, 4, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_emit = (int)(H[0] >> 32), st_red = (int)(H[1] & 0xffffffff);
     if (st_emit) return give_up(fail(st_emit, "ph_tets_emit failed"));
     if (st_red == PH_OK) break;
