@@ -453,6 +453,9 @@ __device__ __forceinline__ u32 sm_xor32(u32* p, u32 x) {
                : "memory");
   return old;
 }
+__device__ __forceinline__ void sm_red_xor32(u32* p, u32 x) {
+  asm volatile("red.shared.xor.b32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(x) : "memory");
+}
 __device__ __forceinline__ void sm_st32(u32* p, u32 v) {
   asm volatile("st.shared.u32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(v) : "memory");
 }
@@ -464,17 +467,18 @@ __device__ __forceinline__ u32 dense_xor(const DenseCol& D, i64 w, u32 b) {
 
 // flips the sorted entries src[0..len) (global ranks); returns the change in
 // the number of set bits (warp-uniform) and widens the touched range
-// flips the sorted entries held one per lane (lanes < len <= 32)
-__device__ int dense_flip_regs(DenseCol& D, i32 v, int len, i32 row_base) {
+// flips the sorted entries held one per lane (lanes < len <= 32); the set-bit
+// count is not tracked here (the flips need not return their old words): a
+// vanished column shows as no set bit at the pivot scan, and the count of a
+// column is taken when it is published
+__device__ void dense_flip_regs(DenseCol& D, i32 v, int len, i32 row_base) {
   const int lane = threadIdx.x & 31;
-  int delta = 0;
   if (lane < len) {
     const i32 e = v - row_base;
     const u32 b = 1u << (e & 31);
-    const u32 old = dense_xor(D, e >> 5, b);
-    delta = (old & b) ? -1 : 1;
+    if (D.sm) sm_red_xor32(D.bits + (e >> 5), b);
+    else atomicXor(D.bits + (e >> 5), b);
   }
-  delta = __reduce_add_sync(FULL, delta);
   const i32 first = __shfl_sync(FULL, v, 0), last = __shfl_sync(FULL, v, (len - 1) & 31);
   if (len > 0) {
     const i64 w0 = (i64)((first - row_base) >> 5), w1 = (i64)((last - row_base) >> 5);
@@ -482,7 +486,14 @@ __device__ int dense_flip_regs(DenseCol& D, i32 v, int len, i32 row_base) {
     D.hi = max(D.hi, w1);
   }
   __syncwarp();
-  return delta;
+}
+
+// set bits of the bitmap (all at or after the pivot's word)
+__device__ int dense_count(const DenseCol& D, i32 row_base) {
+  const int lane = threadIdx.x & 31;
+  int c = 0;
+  for (i64 w = (i64)((D.piv - row_base) >> 5) + lane; w <= D.hi; w += 32) c += __popc(dense_word(D, w));
+  return __reduce_add_sync(FULL, c);
 }
 
 __device__ int dense_flip(DenseCol& D, const i32* src, bool srcg, int len, i32 row_base) {
@@ -660,6 +671,7 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
       if (!take && o < c) {
         // publish W as a record, then claim p
         if (!published) {
+          if (dense) k = dense_count(D, row_base);
           const unsigned long long at = pool_alloc(chunk_state, ctl, pool_cap, k + 1, chunk, status);
           if (at == ~0ull) break;
           if (lane == 0) pool[at] = k;
@@ -688,14 +700,16 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
             // the bitmap holds the claimer's content: flip the displaced record into it
             const u64 at_d = old & OW_OFF;
             const int len_d = __ldcg(pool + at_d);
-            k += dense_flip(D, pool + at_d + 1, true, len_d, row_base);
+            dense_flip(D, pool + at_d + 1, true, len_d, row_base);
             ++n_merges;
             published = false;
-            if (k == 0) {
+            D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+            if (D.piv < 0) {  // the column vanished
+              k = 0;
               leave_dense();
               break;
             }
-            D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+            k = 1;  // nonzero; counted when published
             continue;
           }
           if (!wg) {
@@ -720,14 +734,19 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
       if (!dense && dense_ok && k + lb > RD_CAP) enter_dense(W, wg, k);  // W outgrows its buffer
       if (dense) {
         // entries 0..30 of the added column are already in registers
-        k += lb <= 31 ? dense_flip_regs(D, bv, lb, row_base) : dense_flip(D, pool + at_o + 1, true, lb, row_base);
+        if (lb <= 31)
+          dense_flip_regs(D, bv, lb, row_base);
+        else
+          dense_flip(D, pool + at_o + 1, true, lb, row_base);
         ++n_merges;
         published = false;
-        if (k == 0) {
+        D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+        if (D.piv < 0) {  // the column vanished
+          k = 0;
           leave_dense();
           break;
         }
-        D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+        k = 1;  // nonzero; counted when published
         continue;
       }
       if (!wg && lb <= 31 && k + lb <= RD_CAP) {
