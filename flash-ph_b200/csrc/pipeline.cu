@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -65,27 +66,46 @@ struct Arena {
   }
 };
 
-// small pinned, device-mapped host buffer per thread for count and status
-// readbacks (a kernel writes the values into it directly)
+// Small pinned, device-mapped host buffers for count and status readbacks (a
+// kernel writes the values into them directly). They come from a process-wide
+// pool: a call takes one and returns it, so host threads that come and go (a
+// server's worker slots) do not allocate pinned memory, which can wait for the
+// whole device, on their first call.
 struct Slots {
   int64_t* host = nullptr;
   int64_t* dev = nullptr;
 };
-Slots pinned_slots() {
-  thread_local Slots b;
-  if (!b.host) {
-    void* p = nullptr;
-    if (cudaHostAlloc(&p, 64 * sizeof(int64_t), cudaHostAllocMapped) != cudaSuccess) return Slots{};
-    void* d = nullptr;
-    if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
-      cudaFreeHost(p);
-      return Slots{};
+std::mutex g_slots_mu;
+std::vector<Slots> g_slots_free;
+
+Slots take_slots() {
+  {
+    std::lock_guard<std::mutex> lock(g_slots_mu);
+    if (!g_slots_free.empty()) {
+      const Slots b = g_slots_free.back();
+      g_slots_free.pop_back();
+      return b;
     }
-    b.host = static_cast<int64_t*>(p);
-    b.dev = static_cast<int64_t*>(d);
   }
-  return b;
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, 64 * sizeof(int64_t), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+    return Slots{};
+  void* d = nullptr;
+  if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
+    cudaFreeHost(p);
+    return Slots{};
+  }
+  return Slots{static_cast<int64_t*>(p), static_cast<int64_t*>(d)};
 }
+
+struct SlotsLease {
+  Slots b = take_slots();
+  ~SlotsLease() {
+    if (!b.host) return;
+    std::lock_guard<std::mutex> lock(g_slots_mu);
+    g_slots_free.push_back(b);
+  }
+};
 
 // copies up to four device int64 values into the mapped host slots
 __global__ void k_report(const int64_t* a, const int64_t* b, const int64_t* c, const int64_t* d, int count,
@@ -230,7 +250,8 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   int dev = 0;
   cudaGetDevice(&dev);
   keep_pool(dev);
-  const Slots slots = pinned_slots();
+  const SlotsLease lease;
+  const Slots& slots = lease.b;
   if (!slots.host) return fail(PH_ERR_CUDA, "ph_rips_persistence: pinned host buffer unavailable");
   volatile int64_t* H = slots.host;
 
