@@ -12,6 +12,7 @@
 //      tetrahedron count when H2 is asked for
 //   4. the H2 reduction's status and row count
 // The results stay on the device in a ph_result until copied out.
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -74,7 +75,9 @@ struct Arena {
 struct Slots {
   int64_t* host = nullptr;
   int64_t* dev = nullptr;
+  int64_t* seq = nullptr;  // host-side count of readbacks through this buffer
 };
+constexpr int kSeqSlot = 8;  // word the readback kernel writes last
 std::mutex g_slots_mu;
 std::vector<Slots> g_slots_free;
 
@@ -95,7 +98,10 @@ Slots take_slots() {
     cudaFreeHost(p);
     return Slots{};
   }
-  return Slots{static_cast<int64_t*>(p), static_cast<int64_t*>(d)};
+  Slots b{static_cast<int64_t*>(p), static_cast<int64_t*>(d), nullptr};
+  b.seq = new int64_t(0);
+  static_cast<int64_t*>(p)[kSeqSlot] = 0;
+  return b;
 }
 
 struct SlotsLease {
@@ -109,11 +115,15 @@ struct SlotsLease {
 
 // copies up to four device int64 values into the mapped host slots
 __global__ void k_report(const int64_t* a, const int64_t* b, const int64_t* c, const int64_t* d, int count,
-                         volatile int64_t* out) {
+                         volatile int64_t* out, int64_t seq) {
   ph::pdl_wait();
   ph::pdl_trigger();
   const int64_t* src[4] = {a, b, c, d};
   if (threadIdx.x < count && threadIdx.x < 4) out[threadIdx.x] = *src[threadIdx.x];
+  __threadfence_system();
+  __syncwarp();
+  // the sequence word last: the host reads the values once it sees it
+  if (threadIdx.x == 0) out[kSeqSlot] = seq;
   __threadfence_system();
 }
 
@@ -163,42 +173,38 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-// event per host thread for the readback waits
-cudaEvent_t wait_event() {
-  thread_local cudaEvent_t ev = nullptr;
-  if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) ev = nullptr;
-  return ev;
-}
-
 // brings count (<= 4) int64 values from the device into the pinned slots (one
-// kernel writes them into the mapped host buffer) and waits: polls for up to
-// half a millisecond (the usual wait is a few microseconds, and a blocking
-// wait adds its wake-up latency to every readback), then blocks
+// kernel writes them into the mapped host buffer, then a sequence word) and
+// waits: spins on the sequence word for up to half a millisecond (the usual
+// wait is a few microseconds, and a blocking wait adds its wake-up latency to
+// every readback), then blocks
 int readback(const int64_t* const* src, int count, const Slots& dst, cudaStream_t s) {
+  const int64_t seq = ++*dst.seq;
   count_launch();
   if (ph::launch_pdl(k_report, dim3(1), dim3(32), 0, s, src[0], count > 1 ? src[1] : src[0],
-                     count > 2 ? src[2] : src[0], count > 3 ? src[3] : src[0], count, dst.dev) != cudaSuccess) {
+                     count > 2 ? src[2] : src[0], count > 3 ? src[3] : src[0], count, dst.dev,
+                     seq) != cudaSuccess) {
     record_error(cudaGetLastError());
     return PH_ERR_CUDA;
   }
-  cudaEvent_t ev = wait_event();
-  if (ev && cudaEventRecord(ev, s) == cudaSuccess) {
-    const auto t0 = std::chrono::steady_clock::now();
-    for (;;) {
-      const cudaError_t q = cudaEventQuery(ev);
-      if (q == cudaSuccess) return PH_OK;
-      if (q != cudaErrorNotReady) {
-        record_error(q);
-        return PH_ERR_CUDA;
-      }
-      if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(500)) break;
+  // spin on the sequence word in host memory (no driver call, so concurrent
+  // callers on other threads do not contend for the driver while waiting)
+  volatile int64_t* flag = dst.host + kSeqSlot;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int it = 0;; ++it) {
+    if (*flag == seq) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      return PH_OK;
     }
+    if ((it & 255) == 255 && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(500)) break;
   }
+  // a long stage: block, then the word is there (or the stream reports an error)
   const cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     record_error(e);
     return PH_ERR_CUDA;
   }
+  std::atomic_thread_fence(std::memory_order_acquire);
   return PH_OK;
 }
 
