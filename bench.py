@@ -551,6 +551,19 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(values, world, device):
+    """Each value's maximum over the ranks: the job's time is its slowest
+    replica's. The same collective on every rank (any backend)."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def run_reference(args, world, rank):
     """CPU oracle (port of the reference algorithm) on all host threads."""
     if rank != 0:
@@ -674,10 +687,7 @@ def main():
         d2h = sum(r.numel() * 4 for r in res)
     e2e = statistics.mean(e2e_ms)
 
-    vals = torch.tensor([ms, e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, e2e = (float(x) for x in vals.cpu())
+    ms, e2e = max_over_ranks([ms, e2e], world, dev)
 
     if rank == 0:
         pk, src = peaks()
