@@ -184,7 +184,7 @@ def _plain_stream(reqs, arrivals):
     return np.asarray(done), ok
 
 
-def _served_stream(reqs, arrivals, slots=3):
+def _served_stream(reqs, arrivals, slots=2):
     from flashph_b200.serve import PersistenceServer
     t0 = time.perf_counter()
     done = [0.0] * len(reqs)
@@ -215,9 +215,11 @@ def serving_summary(count, rates_rel=(0.5,), seed=7):
     thr = _thresholds([r[0] for r in reqs])
     for r, t in zip(reqs, thr):
         r[1] = t
-    # warm both paths
-    _plain_stream(reqs[:4], np.zeros(4))
-    _served_stream(reqs[:4], np.zeros(4))
+    # warm both paths over the whole request set: the first pass of a request
+    # mix grows the device memory pool to its peak (for the served path, the
+    # peak of the requests in flight together), a one-time cost of any server
+    _plain_stream(reqs, np.zeros(len(reqs)))
+    _served_stream(reqs, np.zeros(len(reqs)))
     burst = np.zeros(count)
     pd, pok = _plain_stream(reqs, burst)
     sd, sok, nb = _served_stream(reqs, burst)

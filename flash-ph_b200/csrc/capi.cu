@@ -11,10 +11,12 @@ namespace ph {
 namespace {
 thread_local std::string g_last_error;
 std::atomic<unsigned long long> g_launches{0};
+thread_local bool g_dependent_launch = true;
 }  // namespace
 void record_error(cudaError_t e) { g_last_error = cudaGetErrorString(e); }
 void record_message(const char* msg) { g_last_error = msg; }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+bool dependent_launch_enabled() { return g_dependent_launch; }
 // Per-device caches of launch facts that do not change while the process
 // runs (attribute and occupancy queries cost a microsecond or more of host
 // time each, on a path that launches dozens of kernels per call).
@@ -111,3 +113,5 @@ extern "C" const char* ph_last_error(void) { return ph::g_last_error.c_str(); }
 extern "C" unsigned long long ph_launch_count(void) {
   return ph::g_launches.load(std::memory_order_relaxed);
 }
+
+extern "C" void ph_set_dependent_launch(int32_t enable) { ph::g_dependent_launch = enable != 0; }

@@ -57,6 +57,7 @@ _SIGS = {
     "ph_result_stat": (I64, [P, I32]),
     "ph_result_copy": (ctypes.c_int, [P, I32, P, I32, P]),
     "ph_result_copy_all": (ctypes.c_int, [P, P, I32, P]),
+    "ph_set_dependent_launch": (None, [I32]),
     "ph_result_free": (None, [P]),
     "ph_triangles_total_max_vertices": (I64, []),
     "ph_triangles_total": (ctypes.c_int, [P, P, I64, P, P, P]),

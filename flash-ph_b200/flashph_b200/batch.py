@@ -13,10 +13,19 @@ Clouds are processed in chunks bounded by point and pair counts. Errors that
 the reference raises per call (validation, the triangle and tetrahedron
 caps) are returned per cloud as exception objects; they do not stop the
 batch.
+
+Clouds of at least ``NATIVE_MIN_POINTS`` points do not join the chunks: each
+runs as one native pipeline call (``ph_rips_persistence``), two at a time on
+worker streams. The union pipeline pays off where a call's fixed cost (about
+80 short kernels and four host waits) dominates, i.e. for small clouds; for
+larger ones the native call, whose stages are specialised to one cloud and
+chained on the device, is faster.
 """
 from __future__ import annotations
 
 import math
+import threading
+from concurrent.futures import ThreadPoolExecutor
 from typing import Sequence
 
 import numpy as np
@@ -26,6 +35,7 @@ from torch import Tensor
 from . import _lib as L
 from .boruvka import boruvka_mask
 from .cohomology import Reduction, cof_max_face, cofacet_csr, grow_pool, pool_capacity, reduce as _reduce
+from .persistence import _compute_native
 from .rips import edge_filtration_values, threshold_sq, vertex_csr
 
 PH_ERR_POOL = 5
@@ -37,6 +47,36 @@ _CHUNK_POINTS = 1 << 18
 _CHUNK_PAIRS = 1 << 34
 _CHUNK_TRIANGLES = 1 << 28   # per chunk, keeps every global rank in int32
 _CHUNK_TETS = 1 << 28
+NATIVE_MIN_POINTS = 1024  # clouds this large run as native calls
+_NATIVE_WORKERS = 2
+
+
+def _run_native(items, device, max_triangles, max_tetrahedra):
+    """(cloud, points, t, max_dim) items as native calls on worker streams;
+    returns {cloud: diagrams or the reference's exception}."""
+    caller = torch.cuda.current_stream(device)
+    ready = torch.cuda.Event()
+    ready.record(caller)  # inputs written on the caller's stream are complete before the workers read them
+    local = threading.local()
+
+    def one(item):
+        c, p, t, md = item
+        if not hasattr(local, "stream"):
+            local.stream = torch.cuda.Stream(device)
+            local.stream.wait_event(ready)
+        with torch.cuda.device(device), torch.cuda.stream(local.stream):
+            try:
+                x = p.to(device).float().contiguous()
+                out = _compute_native(x, t, md, device, max_triangles, max_tetrahedra)
+                for o in out:
+                    o.record_stream(caller)  # the caller's later use keeps the memory from early reuse
+            except ValueError as ex:  # the reference's per-call errors
+                out = ex
+        local.stream.synchronize()
+        return c, out
+
+    with ThreadPoolExecutor(max_workers=_NATIVE_WORKERS) as ex:
+        return dict(ex.map(one, items))
 
 
 def _validate(points, t, max_dim):
@@ -341,6 +381,12 @@ def rips_persistence_batch(
             results[c] = _trivial(t.shape[0], ds[c], device)
         else:
             todo.append(c)
+    native = [c for c in todo if int(pts[c].shape[0]) >= NATIVE_MIN_POINTS]
+    if native:
+        done = _run_native([(c, pts[c], ts[c], ds[c]) for c in native], device, max_triangles, max_tetrahedra)
+        for c, r in done.items():
+            results[c] = r
+        todo = [c for c in todo if int(pts[c].shape[0]) < NATIVE_MIN_POINTS]
     sizes = {c: int(pts[c].shape[0]) for c in todo}
     work = list(_chunks(todo, sizes))
     while work:

@@ -25,6 +25,7 @@ from concurrent.futures import Future
 import numpy as np
 import torch
 
+from . import _lib as L
 from .batch import rips_persistence_batch
 from .persistence import rips_persistence
 
@@ -54,7 +55,7 @@ class PersistenceServer:
     solo_min_points : requests this large run alone (native pipeline).
     """
 
-    def __init__(self, device=None, slots: int = 3, max_batch_points: int = 1 << 17,
+    def __init__(self, device=None, slots: int = 2, max_batch_points: int = 1 << 17,
                  max_batch_pairs: int = 1 << 32, max_batch_requests: int = 1024,
                  max_triangles: int = 10_000_000, max_tetrahedra: int = 10_000_000,
                  solo_min_points: int = 0):
@@ -117,6 +118,9 @@ class PersistenceServer:
 
     def _worker(self):
         torch.cuda.set_device(self.device)
+        # slots drive their streams concurrently: plain stream order for their
+        # launches (dependently launched blocks would hold SMs while waiting)
+        L.lib().ph_set_dependent_launch(0)
         stream = torch.cuda.Stream(self.device)
         while True:
             with self._cv:

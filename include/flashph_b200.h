@@ -44,6 +44,15 @@ const char* ph_last_error(void);
 /* Number of kernels this library has launched in this process so far. */
 unsigned long long ph_launch_count(void);
 
+/* Kernels launched from the calling host thread are chained with
+ * programmatic dependent launch (the next kernel's blocks are scheduled while
+ * the current one drains; each kernel waits on the device for its
+ * predecessor). On by default; enable = 0 switches it off for this thread,
+ * e.g. for threads that drive several streams at once, where blocks scheduled
+ * early hold SMs that another stream's kernels could use. No counterpart in
+ * the reference (a launch policy of this library). */
+void ph_set_dependent_launch(int32_t enable);
+
 /* ---- filtration -------------------------------------------------------- */
 
 /* One point cloud of a batch. A batch is the disjoint union of its clouds:

@@ -93,3 +93,35 @@ def test_auto_threshold_batch_equals_single():
         k = max(1, min(20, c.shape[0] - 1))
         kth = np.sqrt(np.sort(d2, axis=1)[:, k - 1])
         assert abs(g - np.quantile(kth, 0.95)) <= 1e-5 * max(1.0, abs(g))
+
+
+def test_large_clouds_take_the_native_route_and_match_single_calls():
+    """Clouds on both sides of NATIVE_MIN_POINTS (native calls on worker
+    streams, and the union pipeline), CUDA and host inputs, and a large cloud
+    over the triangle cap: every result equals its single call or the
+    reference's error."""
+    from flashph_b200 import rips_persistence
+    from flashph_b200.batch import NATIVE_MIN_POINTS, rips_persistence_batch
+    rng = np.random.default_rng(17)
+    sizes = [NATIVE_MIN_POINTS - 1, NATIVE_MIN_POINTS, 1500, 300, 2600, 64]
+    clouds, ts, dims = [], [], []
+    for k, n in enumerate(sizes):
+        d = [3, 8, 10][k % 3]
+        clouds.append(rng.standard_normal((n, d)).astype(np.float32))
+        ts.append({3: 0.35, 8: 1.5, 10: 1.9}[d])
+        dims.append(2 if k % 2 == 0 else 1)
+    clouds[4] = torch.from_numpy(clouds[4]).cuda()  # a device input among host ones
+    dense = (rng.standard_normal((1200, 3)) * 0.05).astype(np.float32)
+    clouds.append(dense)
+    ts.append(10.0)
+    dims.append(1)
+    res = rips_persistence_batch(clouds, ts, dims, max_triangles=5_000_000)
+    assert isinstance(res[-1], ValueError) and "max_triangles=5000000" in str(res[-1])
+    for p, t, md, r in zip(clouds[:-1], ts[:-1], dims[:-1], res[:-1]):
+        assert not isinstance(r, Exception), r
+        x = p if isinstance(p, torch.Tensor) else torch.from_numpy(p).cuda()
+        single = rips_persistence(x, t, max_dim=md)
+        assert len(r) == md + 1
+        for dim in range(md + 1):
+            assert r[dim].device.type == "cuda"
+            assert _same(r[dim], single[dim]), (p.shape, dim)
