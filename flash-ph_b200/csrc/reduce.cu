@@ -607,9 +607,10 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
     const int l = __ffs(todo) - 1;
     todo &= todo - 1;
     i32 c = (i32)(K - 1 - base - l);
-    // working column: shared buffer (sW0 + cur * RD_CAP) or, when too long, a pool record
+    // working column: shared buffer (sW0 + cur * RD_CAP), a pool record when too
+    // long, or the bitmap D
     int cur = 0;
-    int k = 0;
+    int k = 0;  // entries of W; for the bitmap only zero/nonzero until it is published
     const i32* W = nullptr;
     bool wg = false;      // W is in global memory
     bool published = false;
