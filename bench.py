@@ -700,7 +700,7 @@ def main():
                                                            "h1.cofacets", "h1.reduce", "h2")}
         dominant = max(leaf, key=leaf.get) if leaf else "edges"
         cpu = None
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the host-core baseline belongs to the one-GPU line
             import oracle
 
             oracle.build()
@@ -732,7 +732,7 @@ def main():
                              "native pipeline",
             "sizes": {"edges": E, "triangles": T},
         }
-        if not args.no_serving:
+        if not args.no_serving and world == 1:  # a one-GPU sub-measurement
             line["serving"] = serving_summary(args.serving_requests, rates_rel=(0.5,))
         print(json.dumps(line), flush=True)
     if world > 1:
