@@ -221,13 +221,20 @@ def serving_summary(count, rates_rel=(0.5,), seed=7):
     _plain_stream(reqs, np.zeros(len(reqs)))
     _served_stream(reqs, np.zeros(len(reqs)))
     burst = np.zeros(count)
-    pd, pok = _plain_stream(reqs, burst)
-    sd, sok, nb = _served_stream(reqs, burst)
-    plain_rate = count / pd.max()
-    served_rate = count / sd.max()
+    # three alternating bursts per path, medians reported (a single burst varies
+    # by tens of percent between runs)
+    plain_rates, served_rates = [], []
+    for _ in range(3):
+        pd, pok = _plain_stream(reqs, burst)
+        sd, sok, nb = _served_stream(reqs, burst)
+        plain_rates.append(count / pd.max())
+        served_rates.append(count / sd.max())
+    plain_rate = float(np.median(plain_rates))
+    served_rate = float(np.median(served_rates))
     out = {"requests": count, "ok": int(sok), "plain_ok": int(pok), "capped_or_invalid": int(count - sok),
            "plain_diagrams_per_s": round(plain_rate, 2), "served_diagrams_per_s": round(served_rate, 2),
            "served_over_plain": round(served_rate / plain_rate, 3), "served_batches_burst": int(nb),
+           "bursts": {"plain": [round(x, 1) for x in plain_rates], "served": [round(x, 1) for x in served_rates]},
            "rates": []}
     rng = np.random.default_rng(seed + 1)
     for rel in rates_rel:

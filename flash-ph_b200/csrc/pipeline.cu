@@ -128,16 +128,19 @@ __global__ void k_report(const int64_t* a, const int64_t* b, const int64_t* c, c
 }
 
 // keeps the device's stream-ordered pool from returning memory at every sync
-// (a setting of this process's pool, nothing that outlasts it)
+// (a setting of this process's pool, nothing that outlasts it). Cross-stream
+// reuse stays at the default (an allocation may wait for another stream's
+// free): turning it off made concurrent serving slower, through pool growth.
 void keep_pool(int dev) {
-  static bool done[64] = {};
-  if (dev < 0 || dev >= 64 || done[dev]) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
-  done[dev] = true;
+  static std::once_flag once[64];
+  if (dev < 0 || dev >= 64) return;
+  std::call_once(once[dev], [dev]() {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  });
 }
 
 // fp32 of a double, round to nearest even, inf beyond the fp32 range (numpy's float32())
