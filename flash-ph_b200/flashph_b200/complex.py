@@ -36,17 +36,24 @@ class RipsComplex:
                                           backend=backend)
 
     def persistence(self, max_dim: int = 1, homology_coeff_field: int = 2):
-        """Compute and return sorted ``(dim, (birth, death))`` pairs."""
+        """Compute and return sorted ``(dim, (birth, death))`` pairs.
+
+        The (dim, birth, death) order is made where the diagrams live, with
+        stable sorts by death, then birth, then dimension, and the pairs come
+        back in one copy (no per-row host work besides building the tuples).
+        """
         self.compute_persistence(max_dim, homology_coeff_field)
-        result = []
-        for dim, dgm in enumerate(self._diagrams):
-            if dgm.numel() == 0:
-                continue
-            arr = dgm.cpu().numpy()
-            for i in range(arr.shape[0]):
-                result.append((dim, (float(arr[i, 0]), float(arr[i, 1]))))
-        result.sort(key=lambda x: (x[0], x[1][0], x[1][1]))
-        return result
+        live = [(k, d) for k, d in enumerate(self._diagrams) if d.numel() > 0]
+        if not live:
+            return []
+        rows = torch.cat([d.double() for _, d in live])
+        dims = torch.cat([torch.full((d.shape[0],), float(k), dtype=torch.float64, device=d.device)
+                          for k, d in live])
+        order = torch.argsort(rows[:, 1], stable=True)
+        order = order[torch.argsort(rows[order, 0], stable=True)]
+        order = order[torch.argsort(dims[order], stable=True)]
+        table = torch.stack([dims[order], rows[order, 0], rows[order, 1]], dim=1).cpu().tolist()
+        return [(int(k), (b, e)) for k, b, e in table]
 
     def persistence_intervals_in_dimension(self, dim: int):
         """(K, 2) float64 array of the intervals of one dimension."""
@@ -61,18 +68,19 @@ class RipsComplex:
     def betti_numbers(self):
         """Number of essential (infinite) classes per dimension."""
         self._check_computed()
-        return [int((d[:, 1] == float("inf")).sum()) if d.numel() > 0 else 0 for d in self._diagrams]
+        return self._counts(lambda d: d[:, 1] == float("inf"))
 
     def persistent_betti_numbers(self, from_value: float, to_value: float):
         """Classes born <= from_value and dying > to_value, per dimension."""
         self._check_computed()
-        out = []
-        for dgm in self._diagrams:
-            if dgm.numel() == 0:
-                out.append(0)
-                continue
-            out.append(int(((dgm[:, 0] <= from_value) & (dgm[:, 1] > to_value)).sum()))
-        return out
+        return self._counts(lambda d: (d[:, 0] <= from_value) & (d[:, 1] > to_value))
+
+    def _counts(self, pred):
+        # one count per dimension, brought back in one copy
+        dev = self._diagrams[0].device
+        counts = torch.stack([pred(d).sum() if d.numel() > 0 else torch.zeros((), dtype=torch.int64, device=dev)
+                              for d in self._diagrams])
+        return [int(c) for c in counts.tolist()]
 
     def num_vertices(self) -> int:
         return self._points.shape[0]

@@ -123,3 +123,20 @@ def test_oracle_orders_colex_collisions_by_emission():
     keys = [((int(np.float32(1.0).view(np.uint32)) << 32) | ((j * (j - 1) // 2 + i) & 0xFFFFFFFF))
             for i, j in got]
     assert len(set(keys)) == 1  # a genuine tie of the packed key
+
+
+def test_ripscomplex_formats_match_a_host_sort():
+    """persistence() orders (dim, (birth, death)) on the diagrams' device with
+    one copy back; the result equals a Python sort of every row, ties and
+    infinite deaths included, and the Betti counts come back per dimension."""
+    inf = float("inf")
+    dgms = [torch.tensor([[0.0, 0.5], [0.0, inf], [0.0, 0.25], [0.0, 0.5], [0.0, inf]]),
+            torch.tensor([[0.3, 0.4], [0.3, 0.35], [0.1, inf], [0.3, 0.4]]),
+            torch.zeros((0, 2))]
+    rc = RipsComplex(torch.zeros(3, 2), 1.0)
+    rc.compute_persistence = lambda *a, **k: None
+    rc._diagrams, rc._max_dim = dgms, 2
+    want = sorted((k, (float(b), float(e))) for k, d in enumerate(dgms) for b, e in d.tolist())
+    assert rc.persistence(max_dim=2) == want
+    assert rc.betti_numbers() == [2, 1, 0]
+    assert rc.persistent_betti_numbers(0.3, 0.36) == [4, 3, 0]
