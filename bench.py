@@ -184,7 +184,7 @@ def _plain_stream(reqs, arrivals):
     return np.asarray(done), ok
 
 
-def _served_stream(reqs, arrivals, slots=2):
+def _served_stream(reqs, arrivals, slots=1):
     from flashph_b200.serve import PersistenceServer
     t0 = time.perf_counter()
     done = [0.0] * len(reqs)

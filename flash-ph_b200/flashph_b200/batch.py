@@ -51,6 +51,22 @@ NATIVE_MIN_POINTS = 1024  # clouds this large run as native calls
 _NATIVE_WORKERS = 2
 
 
+# Worker streams are kept for the life of the process and reused (by the
+# native workers below and by serve.py's slots): torch's caching allocator
+# keeps its free blocks per stream, so fresh streams would start every call
+# with cold caches (fresh device allocations, which can wait for the device).
+_STREAMS: dict = {}
+_STREAMS_LOCK = threading.Lock()
+
+
+def worker_stream(device, index: int):
+    key = (device.index if device.index is not None else torch.cuda.current_device(), index)
+    with _STREAMS_LOCK:
+        if key not in _STREAMS:
+            _STREAMS[key] = torch.cuda.Stream(device)
+        return _STREAMS[key]
+
+
 def _run_native(items, device, max_triangles, max_tetrahedra):
     """(cloud, points, t, max_dim) items as native calls on worker streams;
     returns {cloud: diagrams or the reference's exception}."""
@@ -58,11 +74,15 @@ def _run_native(items, device, max_triangles, max_tetrahedra):
     ready = torch.cuda.Event()
     ready.record(caller)  # inputs written on the caller's stream are complete before the workers read them
     local = threading.local()
+    taken = iter(range(_NATIVE_WORKERS))
+    taken_lock = threading.Lock()
 
     def one(item):
         c, p, t, md = item
         if not hasattr(local, "stream"):
-            local.stream = torch.cuda.Stream(device)
+            with taken_lock:
+                idx = next(taken)
+            local.stream = worker_stream(device, 100 + idx)  # indices apart from the server's slots
             local.stream.wait_event(ready)
         with torch.cuda.device(device), torch.cuda.stream(local.stream):
             try:

@@ -6,8 +6,12 @@ request of at least ``solo_min_points`` points runs alone through the native
 pipeline (``ph_rips_persistence``, one library call that waits on the host
 four times at most); the small requests at the head of the queue that fit
 the admission limits run together as one batch through the batching
-pipeline (``batch.rips_persistence_batch``). While one slot waits on the
-host, another slot's work runs on the GPU. Admission is by memory, estimated
+pipeline (``batch.rips_persistence_batch``), which spreads a call's fixed
+cost over them; a small request with no company runs alone too. Defaults:
+one slot and every request native (``solo_min_points=0``). On the serving
+stream neither several slots (streams at once) nor batching the small
+requests measured faster than one native call at a time, which already keeps
+the GPU busy; both remain available as parameters. Admission is by memory, estimated
 from the request sizes (points, candidate pairs); the pipelines' own
 counting passes enforce the reference's per-call triangle and tetrahedron
 caps per request.
@@ -26,7 +30,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .batch import rips_persistence_batch
+from .batch import rips_persistence_batch, worker_stream as slot_stream
 from .persistence import rips_persistence
 
 
@@ -48,14 +52,15 @@ class PersistenceServer:
 
     Parameters
     ----------
-    slots : concurrent batches in flight (each on its own stream).
+    slots : concurrent batches in flight (each on its own stream; default 1).
     max_batch_points : admission limit on the points of one batch.
     max_batch_pairs : admission limit on candidate point pairs of one batch.
     max_batch_requests : admission limit on requests per batch.
-    solo_min_points : requests this large run alone (native pipeline).
+    solo_min_points : requests this large run alone (native pipeline, the
+        default for all); smaller ones are batched when more than one waits.
     """
 
-    def __init__(self, device=None, slots: int = 2, max_batch_points: int = 1 << 17,
+    def __init__(self, device=None, slots: int = 1, max_batch_points: int = 1 << 17,
                  max_batch_pairs: int = 1 << 32, max_batch_requests: int = 1024,
                  max_triangles: int = 10_000_000, max_tetrahedra: int = 10_000_000,
                  solo_min_points: int = 0):
@@ -72,7 +77,7 @@ class PersistenceServer:
         self._cv = threading.Condition()
         self._closed = False
         self.batches = 0
-        self._workers = [threading.Thread(target=self._worker, daemon=True, name=f"ph-slot-{i}")
+        self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True, name=f"ph-slot-{i}")
                          for i in range(slots)]
         for w in self._workers:
             w.start()
@@ -116,12 +121,13 @@ class PersistenceServer:
             pairs += n * n // 2
         return batch
 
-    def _worker(self):
+    def _worker(self, index: int):
         torch.cuda.set_device(self.device)
-        # slots drive their streams concurrently: plain stream order for their
-        # launches (dependently launched blocks would hold SMs while waiting)
-        L.lib().ph_set_dependent_launch(0)
-        stream = torch.cuda.Stream(self.device)
+        # several slots drive their streams concurrently: plain stream order for
+        # their launches (dependently launched blocks would hold SMs while waiting)
+        if len(self._workers) > 1:
+            L.lib().ph_set_dependent_launch(0)
+        stream = slot_stream(self.device, index)
         while True:
             with self._cv:
                 while not self._queue and not self._closed:
@@ -131,7 +137,7 @@ class PersistenceServer:
                 batch = self._admit()
             try:
                 with torch.cuda.stream(stream):
-                    if len(batch) == 1 and batch[0].n >= self.solo_min_points:
+                    if len(batch) == 1:  # a large request, or a small one with no company: one native call
                         r = batch[0]
                         try:
                             res = [rips_persistence(r.points, r.t, max_dim=r.max_dim)]
