@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(MST_NT) k_mst(const i32* __restrict__ ei, cons
 // between two arrays by round, the idle one being cleared during the hooks.
 // Parents and offers live in global memory: scattered single-word accesses
 // from many blocks are served by the L2 slices in parallel.
-constexpr int MSTC_NT = 1024;
+constexpr int MSTC_NT = 512;
 constexpr int MSTC_B = 2;  // edges per thread and batch (2 walks each)
 constexpr u64 NO_OFFER = ~0ull;
 
