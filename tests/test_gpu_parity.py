@@ -220,3 +220,25 @@ def test_native_pipeline_host_arrays_and_limits():
     dense = rng.standard_normal((400, 3)).astype(np.float32)  # complete graph: C(400, 3) > 10^7 triangles
     with pytest.raises(ValueError, match="exceeds max_triangles=10000000"):
         rips_persistence(torch.from_numpy(dense).cuda(), 100.0, max_dim=1)
+
+
+@pytest.mark.parametrize("n", [450, 500])
+def test_dense_columns_in_global_bitmaps_match_oracle(n):
+    """Dense H1 (d = 50 at the 30th percentile of distances): about 10^6
+    triangle rows, more than a warp's shared bitmap holds, and working columns
+    of 9K-40K entries (the oracle's col_max), longer than the shared list
+    buffers: columns become bitmaps in global memory. Bit for bit against the
+    oracle."""
+    import oracle
+    from flashph_b200 import rips_persistence
+    rng = np.random.default_rng(5)
+    if n == 500:
+        rng.standard_normal((450, 50))  # the same stream as the probe that sized these cases
+    p = rng.standard_normal((n, 50)).astype(np.float32)
+    dd = np.sqrt(((p[:, None, :].astype(np.float64) - p[None]) ** 2).sum(-1))
+    t = float(np.quantile(dd[np.triu_indices(n, 1)], 0.30))
+    ref = oracle.run(p, t, 1, fused=True)
+    assert ref["T"] > 196_608 and ref["col_max"] > 6144
+    got = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=1)
+    assert _same_rows(got[0].cpu(), ref["h0"])
+    assert _same_rows(got[1].cpu(), ref["h1"])
