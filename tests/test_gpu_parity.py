@@ -242,3 +242,21 @@ def test_dense_columns_in_global_bitmaps_match_oracle(n):
     got = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=1)
     assert _same_rows(got[0].cpu(), ref["h0"])
     assert _same_rows(got[1].cpu(), ref["h1"])
+
+
+def test_h2_with_list_columns_matches_oracle():
+    """H2 with 363K tetrahedron rows: more than a warp's shared bitmap holds,
+    so the H2 working columns are sorted lists in shared memory (the
+    broadcast-rank XOR for short added columns); H1 of the same cloud uses
+    the shared bitmaps. H0-H2 against the oracle."""
+    import oracle
+    from flashph_b200 import rips_persistence
+    p = np.random.default_rng(9).standard_normal((200, 20)).astype(np.float32)
+    dd = np.sqrt(((p[:, None, :].astype(np.float64) - p[None]) ** 2).sum(-1))
+    t = float(np.quantile(dd[np.triu_indices(200, 1)], 0.25))
+    ref = oracle.run(p, t, 2, fused=True)
+    assert ref["Q"] > 196_608 and ref["T"] < 196_608
+    got = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=2)
+    assert _same_rows(got[0].cpu(), ref["h0"])
+    assert _same_rows(got[1].cpu(), ref["h1"])
+    assert _same_rows(sorted_rows(got[2].cpu().numpy()), sorted_rows(ref["h2"]))
