@@ -4,6 +4,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <mutex>
 
 namespace ph {
 
@@ -249,6 +250,20 @@ constexpr int RS_WARPS = RS_NT / 32;
 constexpr int RS_ROUNDS_LARGE = 16, RS_ROUNDS_SMALL = 4;
 constexpr i64 RS_SMALL_MAX = i64(1) << 18;
 __host__ __device__ constexpr int rs_tile(int rounds) { return RS_WARPS * 32 * rounds; }
+// Lanes of the warp whose digit equals this lane's: one ballot per bit of a
+// 9-bit digit (bit 8 marks a lane without a key, so such lanes never match a
+// key's digit). Nine ballots issue in fewer cycles than a match-any.
+__device__ __forceinline__ u32 warp_peers(u32 d) {
+  u32 m = FULL;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const u32 v = __ballot_sync(FULL, bit);
+    m &= bit ? v : ~v;
+  }
+  return m;
+}
+
 constexpr u64 LB_AGG = 1ull << 32, LB_PRE = 2ull << 32;
 constexpr int LB_SPIN_LIMIT = 1 << 24;
 
@@ -380,7 +395,7 @@ __global__ void __launch_bounds__(RS_NT) k_os_pass(u64* kA, u32* vA, u64* kB, u3
       const u64 k = key[r];
       const u32 v = val[r];
       const u32 d = ok ? (u32)((k >> shift) & 255u) : 256u;
-      const u32 peers = __match_any_sync(FULL, d);
+      const u32 peers = warp_peers(d);
       const u32 rank = __popc(peers & lt);
       const u32 b = (d < 256u) ? cnt[w][d] : 0u;
       __syncwarp();
@@ -479,6 +494,135 @@ __global__ void k_os_finish(u64* __restrict__ kA, u32* __restrict__ vA, const u6
   }
 }
 
+// Cluster form for sorts of up to CS x CS_MAX_CHUNK keys: one cluster of CS
+// (16 or 8) blocks holds every (key, value) record in shared memory, block r
+// the records at positions [r * chunk, (r + 1) * chunk) of the current order,
+// split into one run per warp. A pass counts the digits of each run, reads the
+// other blocks' digit counts through distributed shared memory, and writes
+// every record straight into the shared memory of the block that holds its
+// new position, one 16-byte store per record. Order is stable: block, warp
+// run, lane. Two cluster barriers a pass and one launch for the whole sort;
+// global memory is touched only by the first load and the last store. A pass
+// whose digit is the same for every key is skipped (every block sees the same
+// counts, so all skip alike).
+constexpr int CS_NT = 512, CS_WARPS = CS_NT / 32;
+constexpr i64 CS_MAX_CHUNK = 6144;
+constexpr bool CS_PDL = true;  // launched as a dependent of the previous kernel
+
+struct __align__(16) SortRec {
+  u64 key;
+  u64 val;  // the value in the low 32 bits
+};
+
+__host__ __device__ constexpr size_t cs_smem_bytes(i64 chunk) {
+  // two record buffers, per-warp digit counts
+  return (size_t)chunk * 2 * sizeof(SortRec) + (size_t)CS_WARPS * 256 * 4;
+}
+
+template <int CS>
+__global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(u64* keys, u32* vals, i64 n, i64 chunk, int p0, int p1) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  extern __shared__ __align__(16) unsigned char cs_smem[];
+  __shared__ u32 wsum[8];
+  __shared__ u32 chist[256];   // this block's digit counts, read by every block
+  __shared__ u32 dstart[256];  // where this block's records of each digit go
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  SortRec* const rbuf = reinterpret_cast<SortRec*>(cs_smem);
+  u32* const whist = reinterpret_cast<u32*>(rbuf + 2 * chunk);  // [CS_WARPS][256]
+  const i64 lo = (i64)rank * chunk;
+  const int cnt = (int)max((i64)0, min(chunk, n - lo));
+  const int sub = ((cnt + CS_NT - 1) / CS_NT) * 32;  // records per warp run
+  const int wb = min(cnt, w * sub), we = min(cnt, wb + sub);
+  u32* const myh = whist + w * 256;
+  const u32 lt = lanemask_lt();
+  for (int i = tid; i < cnt; i += CS_NT) rbuf[i] = SortRec{keys[lo + i], (u64)vals[lo + i]};
+  int cur = 0;
+  __syncthreads();
+  for (int p = p0; p < p1; ++p) {
+    const int sh = 8 * p;
+    SortRec* const R = rbuf + cur * chunk;
+    for (int i = lane; i < 256; i += 32) myh[i] = 0;
+    __syncwarp();
+    for (int b = wb; b < we; b += 32) {
+      const int i = b + lane;
+      const u32 d = i < we ? (u32)(R[i].key >> sh) & 255u : 256u + lane;
+      const u32 peers = warp_peers(d);
+      if (d < 256u && (peers & lt) == 0) myh[d] += __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+    if (tid < 256) {
+      u32 run = 0;
+      for (int v = 0; v < CS_WARPS; ++v) {
+        const u32 c = whist[v * 256 + tid];
+        whist[v * 256 + tid] = run;
+        run += c;
+      }
+      chist[tid] = run;
+    }
+    cl.sync();  // every block's counts are published
+    bool ident = false;
+    u32 gs = 0;
+    if (tid < 256) {
+      // digit d = tid: its count over the cluster and over the blocks before this one
+      u32 c[CS];
+#pragma unroll
+      for (int r = 0; r < CS; ++r) c[r] = *cl.map_shared_rank(chist + tid, r);
+      u32 tot = 0, below = 0;
+#pragma unroll
+      for (int r = 0; r < CS; ++r) {
+        tot += c[r];
+        if (r < rank) below += c[r];
+      }
+      ident = tot == (u32)n;
+      u32 x = tot;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wsum[w] = x;
+      gs = x - tot + below;
+    }
+    __syncthreads();
+    if (tid < 256) {
+      for (int v = 0; v < w; ++v) gs += wsum[v];
+      dstart[tid] = gs;
+    }
+    const bool skip = __syncthreads_or(ident);
+    if (!skip) {
+      SortRec* const D = rbuf + (cur ^ 1) * chunk;
+      for (int b = wb; b < we; b += 32) {
+        const int i = b + lane;
+        const bool ok = i < we;
+        const SortRec r0 = ok ? R[i] : SortRec{0ull, 0ull};
+        const u32 d = ok ? (u32)(r0.key >> sh) & 255u : 256u + lane;
+        const u32 peers = warp_peers(d);
+        u32 pos = 0;
+        if (ok) pos = dstart[d] + myh[d] + __popc(peers & lt);
+        __syncwarp();
+        if (ok && (peers & lt) == 0) myh[d] += __popc(peers);
+        if (ok && (i64)pos < n) {
+          const int r = (int)(pos / (u32)chunk);
+          *cl.map_shared_rank(D + (pos - (u32)r * (u32)chunk), r) = r0;
+        }
+        __syncwarp();
+      }
+      cur ^= 1;
+    }
+    cl.sync();  // every record is in place; the counts may be rewritten
+  }
+  const SortRec* const R = rbuf + cur * chunk;
+  for (int i = tid; i < cnt; i += CS_NT) {
+    const SortRec r0 = R[i];
+    keys[lo + i] = r0.key;
+    vals[lo + i] = (u32)r0.val;
+  }
+}
+
 }  // namespace
 
 size_t scan_workspace_bytes(i64 n) {
@@ -498,6 +642,39 @@ int scan_exclusive_u8_i32(const uint8_t* in, i32* out, i64 n, void* ws, size_t w
 
 namespace {
 int rs_rounds(i64 n) { return n <= RS_SMALL_MAX ? RS_ROUNDS_SMALL : RS_ROUNDS_LARGE; }
+
+// Blocks in the cluster form's cluster on this device: 16 where a 16-block
+// cluster with full-size buffers can be resident, else 8, 0 when neither can.
+int sort_cluster_size() {
+  static int cached = -1;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cached = 0;
+    for (int cs : {16, 8}) {
+      const void* f = cs == 16 ? (const void*)k_cluster_sort<16> : (const void*)k_cluster_sort<8>;
+      if (allow_dynamic_smem(f) != cudaSuccess) break;
+      if (cs == 16) cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cs;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(CS_NT);
+      cfg.dynamicSmemBytes = cs_smem_bytes(CS_MAX_CHUNK);
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, f, &cfg) == cudaSuccess && clusters > 0) {
+        cached = cs;
+        break;
+      }
+    }
+    cudaGetLastError();
+  });
+  return cached;
+}
 }  // namespace
 
 size_t radix_sort_workspace_bytes(i64 n) {
@@ -513,6 +690,30 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
       begin_bit > end_bit)
     return PH_ERR_ARG;
   if (n <= 1 || begin_bit == end_bit) return PH_OK;
+  const int p0 = begin_bit / 8, p1 = end_bit / 8;
+  const int cs = n <= 16 * CS_MAX_CHUNK ? sort_cluster_size() : 0;
+  if (cs > 0 && n <= cs * CS_MAX_CHUNK) {
+    const i64 chunk = (n + cs - 1) / cs;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(CS_NT);
+    cfg.dynamicSmemBytes = cs_smem_bytes(chunk);
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = CS_PDL && dependent_launch_enabled() ? 2 : 1;
+    ph::count_launch();
+    const cudaError_t e = cs == 16 ? cudaLaunchKernelEx(&cfg, k_cluster_sort<16>, keys, vals, n, chunk, p0, p1)
+                                   : cudaLaunchKernelEx(&cfg, k_cluster_sort<8>, keys, vals, n, chunk, p0, p1);
+    if (e != cudaSuccess) return PH_ERR_CUDA;
+    return PH_OK;
+  }
   const int rounds = rs_rounds(n);
   const i64 tile = rs_tile(rounds);
   const i64 ntiles = (n + tile - 1) / tile;
@@ -525,7 +726,6 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
   // ctl and lb are adjacent in the workspace: one memset clears both
   const size_t clear = (size_t)((char*)(lb + ntiles * 256) - (char*)ctl);
   ph::zero_async(ctl, clear, s);
-  const int p0 = begin_bit / 8, p1 = end_bit / 8;
   const int gh = (int)std::max<i64>(1, std::min<i64>((n + RS_NT * 4 - 1) / (RS_NT * 4), 592));
   ph::count_launch();
   ph::launch_pdl(k_os_hist, dim3(gh), dim3(RS_NT), 0, s, keys, n, p0, p1, ctl);

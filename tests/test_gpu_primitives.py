@@ -23,7 +23,7 @@ def _random_edges(E, n, seed):
     return i.astype(np.int32), j.astype(np.int32), dsq
 
 
-@pytest.mark.parametrize("E", [1, 2, 5, 4095, 4096, 4097, 70000, 1 << 20])
+@pytest.mark.parametrize("E", [1, 2, 5, 17, 4095, 4096, 4097, 70000, 98304, 98305, 1 << 20])
 def test_edges_sort_matches_numpy(E):
     from flashph_b200.rips import sort_edges
     n = 50000
