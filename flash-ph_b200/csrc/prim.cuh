@@ -1,7 +1,10 @@
 // Device-wide primitives written for this library: exclusive scan and a
 // stable LSD radix sort of (u64 key, u32 value) pairs. Both run entirely on
 // the stream with no host synchronisation: the sort decides on the device
-// which 8-bit digits vary and skips the passes of constant digits.
+// which 8-bit digits vary and skips the passes of constant digits. Sorts of
+// up to 98,304 records (16-block clusters; 49,152 with 8) run as one cluster
+// launch that keeps every pass in distributed shared memory; larger ones run
+// one-sweep passes through global memory.
 #pragma once
 #include "common.cuh"
 
