@@ -509,6 +509,7 @@ def kernel_breakdown(pts, t, max_dim, flush, reps=3):
 NCU_TRAFFIC = {
     "k_tc_edges": {"bytes": 2.29e6 + 0.02e6, "source": "profiles/k_tc_edges_20k_d10.md"},
     "k_reduce": {"bytes": 0.83e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
+    "k_cluster_sort": {"bytes": 0.391e6, "source": "profiles/k_cluster_sort_20k_d10.md"},
 }
 
 
@@ -531,9 +532,12 @@ def rooflines(stages, edge_ms, n, d, E, T, pk, src):
     if "sort" in stages:
         byts = 2.0 * 12 * E
         gbs = byts / (stages["sort"] * 1e-3) / 1e9
-        out["sort"] = {"kernel": "filtration sort (k_os_hist, 8 x k_os_pass, k_os_finish)", "bound": "hbm",
+        out["sort"] = {"kernel": "filtration sort (k_edge_keys, one k_cluster_sort launch of 8 digit passes, "
+                                 "k_gather_edges)", "bound": "hbm",
                        "achieved": round(gbs, 2), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 5),
-                       "traffic": None, "algorithmic_bytes_per_launch": byts,
+                       "traffic": NCU_TRAFFIC["k_cluster_sort"]["bytes"],
+                       "traffic_source": NCU_TRAFFIC["k_cluster_sort"]["source"],
+                       "algorithmic_bytes_per_launch": byts,
                        "avg_launch_ms": round(stages["sort"], 5),
                        "per_unit": "12 bytes (i, j, dist^2) read and written per edge",
                        "peak_source": f"hbm_gbs ({src} peaks file)"}
