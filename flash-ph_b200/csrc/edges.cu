@@ -306,6 +306,8 @@ extern "C" int ph_edges_sort(const int32_t* in_i, const int32_t* in_j, const flo
   cudaStream_t s = (cudaStream_t)stream;
   if (E < 0 || E >= (int64_t(1) << 31)) return PH_ERR_OVERFLOW;
   if (E == 0) return PH_OK;
+  const int rc = ph::cluster_sort_edges(in_i, in_j, in_dsq, E, n, out_i, out_j, out_dsq, s);
+  if (rc != ph::CLUSTER_SORT_NA) return rc;
   Carve c(workspace, workspace_bytes);
   u64* keys = c.take<u64>(E);
   u32* vals = c.take<u32>(E);

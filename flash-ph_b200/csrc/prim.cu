@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 namespace ph {
 
@@ -513,14 +514,43 @@ struct __align__(16) SortRec {
   u64 key;
   u64 val;  // the value in the low 32 bits
 };
+__device__ __forceinline__ u64 rec_key(const SortRec& r) { return r.key; }
+__device__ __forceinline__ u64 rec_key(u64 r) { return r; }
 
-__host__ __device__ constexpr size_t cs_smem_bytes(i64 chunk) {
+// What a cluster sort reads and writes: (key, value) pairs sorted in place
+// (16-byte records), or edges (i, j, dist^2) read from ei/ej/dsq and written
+// sorted to oi/oj/od (8-byte records: the packed filtration key
+// bits(dist^2) << 32 | j(j-1)/2 + i, from which the edge is rebuilt; exact
+// while j(j-1)/2 + i < 2^32, that is for n <= 92682).
+struct ClusterSortIO {
+  u64* keys;
+  u32* vals;
+  const i32* ei;
+  const i32* ej;
+  const float* dsq;
+  i32* oi;
+  i32* oj;
+  float* od;
+};
+
+__host__ __device__ constexpr size_t cs_smem_bytes(i64 chunk, size_t rec_bytes) {
   // two record buffers, per-warp digit counts
-  return (size_t)chunk * 2 * sizeof(SortRec) + (size_t)CS_WARPS * 256 * 4;
+  return (size_t)chunk * 2 * rec_bytes + (size_t)CS_WARPS * 256 * 4;
 }
 
-template <int CS>
-__global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(u64* keys, u32* vals, i64 n, i64 chunk, int p0, int p1) {
+__device__ __forceinline__ void edge_of_key(u64 key, i32* i, i32* j, float* d) {
+  const u64 c = key & 0xffffffffull;
+  u64 jj = (u64)((1.0 + sqrt(1.0 + 8.0 * (double)c)) * 0.5);  // j(j-1)/2 <= c < j(j+1)/2
+  while (jj > 1 && jj * (jj - 1) / 2 > c) --jj;
+  while ((jj + 1) * jj / 2 <= c) ++jj;
+  *j = (i32)jj;
+  *i = (i32)(c - jj * (jj - 1) / 2);
+  *d = __uint_as_float((u32)(key >> 32));
+}
+
+template <int CS, bool EDGES>
+__global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(ClusterSortIO io, i64 n, i64 chunk, int p0, int p1) {
+  using Rec = typename std::conditional<EDGES, u64, SortRec>::type;
   ph::pdl_wait();
   ph::pdl_trigger();
   extern __shared__ __align__(16) unsigned char cs_smem[];
@@ -530,7 +560,7 @@ __global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(u64* keys, u32* vals,
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
   const int rank = (int)cl.block_rank();
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  SortRec* const rbuf = reinterpret_cast<SortRec*>(cs_smem);
+  Rec* const rbuf = reinterpret_cast<Rec*>(cs_smem);
   u32* const whist = reinterpret_cast<u32*>(rbuf + 2 * chunk);  // [CS_WARPS][256]
   const i64 lo = (i64)rank * chunk;
   const int cnt = (int)max((i64)0, min(chunk, n - lo));
@@ -538,17 +568,24 @@ __global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(u64* keys, u32* vals,
   const int wb = min(cnt, w * sub), we = min(cnt, wb + sub);
   u32* const myh = whist + w * 256;
   const u32 lt = lanemask_lt();
-  for (int i = tid; i < cnt; i += CS_NT) rbuf[i] = SortRec{keys[lo + i], (u64)vals[lo + i]};
+  for (int i = tid; i < cnt; i += CS_NT) {
+    if constexpr (EDGES) {
+      const u64 a = (u64)io.ei[lo + i], b = (u64)io.ej[lo + i];
+      rbuf[i] = ((u64)__float_as_uint(io.dsq[lo + i]) << 32) | ((b * (b - 1) / 2 + a) & 0xffffffffull);
+    } else {
+      rbuf[i] = SortRec{io.keys[lo + i], (u64)io.vals[lo + i]};
+    }
+  }
   int cur = 0;
   __syncthreads();
   for (int p = p0; p < p1; ++p) {
     const int sh = 8 * p;
-    SortRec* const R = rbuf + cur * chunk;
+    Rec* const R = rbuf + cur * chunk;
     for (int i = lane; i < 256; i += 32) myh[i] = 0;
     __syncwarp();
     for (int b = wb; b < we; b += 32) {
       const int i = b + lane;
-      const u32 d = i < we ? (u32)(R[i].key >> sh) & 255u : 256u + lane;
+      const u32 d = i < we ? (u32)(rec_key(R[i]) >> sh) & 255u : 256u + lane;
       const u32 peers = warp_peers(d);
       if (d < 256u && (peers & lt) == 0) myh[d] += __popc(peers);
       __syncwarp();
@@ -594,12 +631,12 @@ __global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(u64* keys, u32* vals,
     }
     const bool skip = __syncthreads_or(ident);
     if (!skip) {
-      SortRec* const D = rbuf + (cur ^ 1) * chunk;
+      Rec* const D = rbuf + (cur ^ 1) * chunk;
       for (int b = wb; b < we; b += 32) {
         const int i = b + lane;
         const bool ok = i < we;
-        const SortRec r0 = ok ? R[i] : SortRec{0ull, 0ull};
-        const u32 d = ok ? (u32)(r0.key >> sh) & 255u : 256u + lane;
+        const Rec r0 = ok ? R[i] : Rec{};
+        const u32 d = ok ? (u32)(rec_key(r0) >> sh) & 255u : 256u + lane;
         const u32 peers = warp_peers(d);
         u32 pos = 0;
         if (ok) pos = dstart[d] + myh[d] + __popc(peers & lt);
@@ -615,11 +652,14 @@ __global__ void __launch_bounds__(CS_NT, 1) k_cluster_sort(u64* keys, u32* vals,
     }
     cl.sync();  // every record is in place; the counts may be rewritten
   }
-  const SortRec* const R = rbuf + cur * chunk;
+  const Rec* const R = rbuf + cur * chunk;
   for (int i = tid; i < cnt; i += CS_NT) {
-    const SortRec r0 = R[i];
-    keys[lo + i] = r0.key;
-    vals[lo + i] = (u32)r0.val;
+    if constexpr (EDGES) {
+      edge_of_key(R[i], io.oi + lo + i, io.oj + lo + i, io.od + lo + i);
+    } else {
+      io.keys[lo + i] = R[i].key;
+      io.vals[lo + i] = (u32)R[i].val;
+    }
   }
 }
 
@@ -650,10 +690,17 @@ int sort_cluster_size() {
   static std::once_flag once;
   std::call_once(once, [] {
     cached = 0;
+    const void* fs[4] = {(const void*)k_cluster_sort<16, false>, (const void*)k_cluster_sort<16, true>,
+                         (const void*)k_cluster_sort<8, false>, (const void*)k_cluster_sort<8, true>};
+    for (const void* f : fs) {
+      if (allow_dynamic_smem(f) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+      }
+    }
+    cudaFuncSetAttribute(fs[0], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(fs[1], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     for (int cs : {16, 8}) {
-      const void* f = cs == 16 ? (const void*)k_cluster_sort<16> : (const void*)k_cluster_sort<8>;
-      if (allow_dynamic_smem(f) != cudaSuccess) break;
-      if (cs == 16) cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       cudaLaunchConfig_t cfg = {};
       cudaLaunchAttribute at[1];
       at[0].id = cudaLaunchAttributeClusterDimension;
@@ -662,11 +709,11 @@ int sort_cluster_size() {
       at[0].val.clusterDim.z = 1;
       cfg.gridDim = dim3(cs);
       cfg.blockDim = dim3(CS_NT);
-      cfg.dynamicSmemBytes = cs_smem_bytes(CS_MAX_CHUNK);
+      cfg.dynamicSmemBytes = cs_smem_bytes(CS_MAX_CHUNK, sizeof(SortRec));
       cfg.attrs = at;
       cfg.numAttrs = 1;
       int clusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&clusters, f, &cfg) == cudaSuccess && clusters > 0) {
+      if (cudaOccupancyMaxActiveClusters(&clusters, cs == 16 ? fs[0] : fs[2], &cfg) == cudaSuccess && clusters > 0) {
         cached = cs;
         break;
       }
@@ -675,7 +722,47 @@ int sort_cluster_size() {
   });
   return cached;
 }
+
+// One cluster launch sorting n records by digits [p0, p1); CLUSTER_SORT_NA
+// when n is beyond the cluster form (the caller then takes another form).
+template <bool EDGES>
+int cluster_sort(const ClusterSortIO& io, i64 n, int p0, int p1, cudaStream_t s) {
+  const int cs = n <= 16 * CS_MAX_CHUNK ? sort_cluster_size() : 0;
+  if (cs == 0 || n > cs * CS_MAX_CHUNK) return CLUSTER_SORT_NA;
+  const i64 chunk = (n + cs - 1) / cs;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(CS_NT);
+  cfg.dynamicSmemBytes = cs_smem_bytes(chunk, EDGES ? sizeof(u64) : sizeof(SortRec));
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = CS_PDL && dependent_launch_enabled() ? 2 : 1;
+  ph::count_launch();
+  const cudaError_t e = cs == 16 ? cudaLaunchKernelEx(&cfg, k_cluster_sort<16, EDGES>, io, n, chunk, p0, p1)
+                                 : cudaLaunchKernelEx(&cfg, k_cluster_sort<8, EDGES>, io, n, chunk, p0, p1);
+  return e == cudaSuccess ? PH_OK : PH_ERR_CUDA;
+}
 }  // namespace
+
+int cluster_sort_edges(const i32* ei, const i32* ej, const float* dsq, i64 E, i64 n, i32* oi, i32* oj,
+                       float* od, cudaStream_t s) {
+  if (E < 1 || n > 92682) return CLUSTER_SORT_NA;
+  ClusterSortIO io = {};
+  io.ei = ei;
+  io.ej = ej;
+  io.dsq = dsq;
+  io.oi = oi;
+  io.oj = oj;
+  io.od = od;
+  return cluster_sort<true>(io, E, 0, 8, s);
+}
 
 size_t radix_sort_workspace_bytes(i64 n) {
   const i64 tile = rs_tile(rs_rounds(n));
@@ -691,28 +778,12 @@ int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, vo
     return PH_ERR_ARG;
   if (n <= 1 || begin_bit == end_bit) return PH_OK;
   const int p0 = begin_bit / 8, p1 = end_bit / 8;
-  const int cs = n <= 16 * CS_MAX_CHUNK ? sort_cluster_size() : 0;
-  if (cs > 0 && n <= cs * CS_MAX_CHUNK) {
-    const i64 chunk = (n + cs - 1) / cs;
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[2];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = cs;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[1].val.programmaticStreamSerializationAllowed = 1;
-    cfg.gridDim = dim3(cs);
-    cfg.blockDim = dim3(CS_NT);
-    cfg.dynamicSmemBytes = cs_smem_bytes(chunk);
-    cfg.stream = s;
-    cfg.attrs = at;
-    cfg.numAttrs = CS_PDL && dependent_launch_enabled() ? 2 : 1;
-    ph::count_launch();
-    const cudaError_t e = cs == 16 ? cudaLaunchKernelEx(&cfg, k_cluster_sort<16>, keys, vals, n, chunk, p0, p1)
-                                   : cudaLaunchKernelEx(&cfg, k_cluster_sort<8>, keys, vals, n, chunk, p0, p1);
-    if (e != cudaSuccess) return PH_ERR_CUDA;
-    return PH_OK;
+  {
+    ClusterSortIO io = {};
+    io.keys = keys;
+    io.vals = vals;
+    const int rc = cluster_sort<false>(io, n, p0, p1, s);
+    if (rc != CLUSTER_SORT_NA) return rc;
   }
   const int rounds = rs_rounds(n);
   const i64 tile = rs_tile(rounds);

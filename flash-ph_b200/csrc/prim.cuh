@@ -24,6 +24,15 @@ size_t radix_sort_workspace_bytes(i64 n);
 int radix_sort_pairs(u64* keys, u32* vals, i64 n, int begin_bit, int end_bit, void* ws,
                      size_t ws_bytes, cudaStream_t s);
 
+// Edges (i, j, dist^2), i < j < n, sorted by the packed filtration key
+// bits(dist^2) << 32 | j(j-1)/2 + i into oi/oj/od in one cluster launch: the
+// key is built on load and the edge rebuilt from it on store. Returns
+// CLUSTER_SORT_NA (nothing launched) when E is beyond the cluster form or
+// n > 92682 (the packed key is then truncated and ties need emission order).
+constexpr int CLUSTER_SORT_NA = -1;
+int cluster_sort_edges(const i32* ei, const i32* ej, const float* dsq, i64 E, i64 n, i32* oi, i32* oj,
+                       float* od, cudaStream_t s);
+
 // Persistence rows in the reference's order without a sort (batch.cu);
 // col_off (nsegs+1 column offsets) may be null for a single segment.
 size_t rows_nosort_workspace_bytes(i64 K);
