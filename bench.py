@@ -532,11 +532,13 @@ def rooflines(stages, edge_ms, n, d, E, T, pk, src):
     if "sort" in stages:
         byts = 2.0 * 12 * E
         gbs = byts / (stages["sort"] * 1e-3) / 1e9
-        out["sort"] = {"kernel": "filtration sort (k_edge_keys, one k_cluster_sort launch of 8 digit passes, "
-                                 "k_gather_edges)", "bound": "hbm",
+        out["sort"] = {"kernel": "filtration sort (one fused k_cluster_sort launch: packed keys built on load, "
+                                 "8 digit passes, edges rebuilt on store)", "bound": "hbm",
                        "achieved": round(gbs, 2), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 5),
                        "traffic": NCU_TRAFFIC["k_cluster_sort"]["bytes"],
                        "traffic_source": NCU_TRAFFIC["k_cluster_sort"]["source"],
+                       "traffic_note": "captured on the (key, value) form of the same sort: the same 12 bytes "
+                                       "per edge are read once",
                        "algorithmic_bytes_per_launch": byts,
                        "avg_launch_ms": round(stages["sort"], 5),
                        "per_unit": "12 bytes (i, j, dist^2) read and written per edge",
