@@ -16,6 +16,8 @@
 // instead of spinning.
 #include <cooperative_groups.h>
 
+#include <mutex>
+
 #include <algorithm>
 #include <climits>
 
@@ -313,12 +315,23 @@ __global__ void k_h0_rows(const float* __restrict__ filt, const uint8_t* __restr
 
 using namespace ph;
 
-// Cluster size of the cluster form on this device (16 where a 16-block
-// cluster of this kernel can be resident, else 8, 0 when neither can).
+// Cluster size of the cluster form on the current device (16 where a 16-block
+// cluster of this kernel can be resident, else 8, 0 when neither can). The
+// function attribute belongs to a device, so it is set, and the answer
+// cached, once per device.
 int cluster_size() {
-  static int cached = -1;
-  if (cached >= 0) return cached;
-  cached = 0;
+  static std::mutex mu;
+  static int cached[64];
+  static bool known[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 0;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (known[dev]) return cached[dev];
+  known[dev] = true;
+  cached[dev] = 0;
   cudaFuncSetAttribute((const void*)k_mst_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   for (int cs : {16, 8}) {
     cudaLaunchConfig_t cfg = {};
@@ -333,12 +346,12 @@ int cluster_size() {
     cfg.numAttrs = 1;
     int clusters = 0;
     if (cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_mst_cluster, &cfg) == cudaSuccess && clusters > 0) {
-      cached = cs;
+      cached[dev] = cs;
       break;
     }
   }
   cudaGetLastError();
-  return cached;
+  return cached[dev];
 }
 
 extern "C" size_t ph_boruvka_workspace_bytes(int64_t n, int64_t E) {

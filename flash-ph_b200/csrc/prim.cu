@@ -683,44 +683,53 @@ int scan_exclusive_u8_i32(const uint8_t* in, i32* out, i64 n, void* ws, size_t w
 namespace {
 int rs_rounds(i64 n) { return n <= RS_SMALL_MAX ? RS_ROUNDS_SMALL : RS_ROUNDS_LARGE; }
 
-// Blocks in the cluster form's cluster on this device: 16 where a 16-block
-// cluster with full-size buffers can be resident, else 8, 0 when neither can.
+// Blocks in the cluster form's cluster on the current device: 16 where a
+// 16-block cluster with full-size buffers can be resident, else 8, 0 when
+// neither can. Function attributes belong to a device, so they are set, and
+// the answer cached, once per device.
 int sort_cluster_size() {
-  static int cached = -1;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    cached = 0;
-    const void* fs[4] = {(const void*)k_cluster_sort<16, false>, (const void*)k_cluster_sort<16, true>,
-                         (const void*)k_cluster_sort<8, false>, (const void*)k_cluster_sort<8, true>};
-    for (const void* f : fs) {
-      if (allow_dynamic_smem(f) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-      }
-    }
-    cudaFuncSetAttribute(fs[0], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    cudaFuncSetAttribute(fs[1], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    for (int cs : {16, 8}) {
-      cudaLaunchConfig_t cfg = {};
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = cs;
-      at[0].val.clusterDim.y = 1;
-      at[0].val.clusterDim.z = 1;
-      cfg.gridDim = dim3(cs);
-      cfg.blockDim = dim3(CS_NT);
-      cfg.dynamicSmemBytes = cs_smem_bytes(CS_MAX_CHUNK, sizeof(SortRec));
-      cfg.attrs = at;
-      cfg.numAttrs = 1;
-      int clusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&clusters, cs == 16 ? fs[0] : fs[2], &cfg) == cudaSuccess && clusters > 0) {
-        cached = cs;
-        break;
-      }
-    }
+  static std::mutex mu;
+  static int cached[64];
+  static bool known[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
     cudaGetLastError();
-  });
-  return cached;
+    return 0;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (known[dev]) return cached[dev];
+  known[dev] = true;
+  cached[dev] = 0;
+  const void* fs[4] = {(const void*)k_cluster_sort<16, false>, (const void*)k_cluster_sort<16, true>,
+                       (const void*)k_cluster_sort<8, false>, (const void*)k_cluster_sort<8, true>};
+  for (const void* f : fs) {
+    if (allow_dynamic_smem(f) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+  }
+  cudaFuncSetAttribute(fs[0], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaFuncSetAttribute(fs[1], cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  for (int cs : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(CS_NT);
+    cfg.dynamicSmemBytes = cs_smem_bytes(CS_MAX_CHUNK, sizeof(SortRec));
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, cs == 16 ? fs[0] : fs[2], &cfg) == cudaSuccess && clusters > 0) {
+      cached[dev] = cs;
+      break;
+    }
+  }
+  cudaGetLastError();
+  return cached[dev];
 }
 
 // One cluster launch sorting n records by digits [p0, p1); CLUSTER_SORT_NA
