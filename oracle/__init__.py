@@ -22,7 +22,8 @@ ARRAYS = ("edge_i", "edge_j", "edge_dsq", "mst_idx", "h0", "tri_max_rank_sorted"
           "ap_births", "ap_deaths", "res_births", "res_deaths", "ess_births",
           "h1_all_pivots", "h1", "h2", "h2_births", "h2_deaths", "h2_ess")
 SCALARS = ("E", "n_components", "T", "Q", "cofacet_nnz", "n_apparent", "residual", "xor_ops",
-           "xor_max", "xor_elems", "crit_path", "col_max")
+           "xor_max", "xor_elems", "crit_path", "col_max", "E_full", "collapse_removed",
+           "collapse_delayed")
 
 
 def build(force: bool = False) -> str:
@@ -43,6 +44,9 @@ def _load():
                                    ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                    ctypes.c_int64]
+        lib.oracle_run_collapsed.restype = ctypes.c_void_p
+        lib.oracle_run_collapsed.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.oracle_error.restype = ctypes.c_char_p
         lib.oracle_error.argtypes = [ctypes.c_void_p]
         lib.oracle_free.argtypes = [ctypes.c_void_p]
@@ -82,6 +86,28 @@ def run(points, max_edge_length: float, max_dim: int = 1, fused: bool = True,
                        int(max_dim), int(bool(fused)), int(nthreads), int(stop_after),
                        None if ov is None or ov.size == 0 else ov.ctypes.data,
                        -1 if ov is None else ov.size)
+    return _collect(lib, h)
+
+
+def run_collapsed(points, max_edge_length: float, max_dim: int = 2, fused: bool = True,
+                  nthreads: int = 0) -> dict:
+    """The oracle pipeline on the edge-collapsed flag filtration (the step
+    giotto-ph takes before its reduction in the reference's H2 path,
+    persistence.py:48-51). Same keys as ``run``; ``edge_i``/``edge_j`` are
+    the collapsed filtration's edges, ``E_full`` the uncollapsed edge count,
+    ``collapse_removed``/``collapse_delayed`` what the collapse did. Small
+    inputs only (n <= 4096)."""
+    lib = _load()
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+    if pts.ndim != 2:
+        raise ValueError("points must be (n, d)")
+    n, d = pts.shape
+    h = lib.oracle_run_collapsed(pts.ctypes.data if n else None, n, d, float(max_edge_length),
+                                 int(max_dim), int(bool(fused)), int(nthreads))
+    return _collect(lib, h)
+
+
+def _collect(lib, h) -> dict:
     try:
         err = lib.oracle_error(h)
         if err:

@@ -8,6 +8,7 @@
 //
 // Build: make -C oracle   (produces oracle/_build/libph_oracle.so)
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -47,6 +48,9 @@ struct Result {
   i64 Q = 0;
   std::vector<float> h2;
   std::vector<i32> h2_births, h2_deaths, h2_ess;
+  // edge collapse (oracle_run_collapsed): edges of the full filtration, edges
+  // dropped, edges inserted later than their own time
+  i64 E_full = 0, collapse_removed = 0, collapse_delayed = 0;
   std::string error;
 };
 
@@ -585,6 +589,114 @@ void h2_blocks(Result& R, const CSR& g, const Triangles& tr, const std::vector<f
 
 }  // namespace
 
+// --- Edge collapse of the flag filtration -------------------------------
+// The reference computes H2 with giotto-ph's ripser_parallel(...,
+// collapse_edges=True) (persistence.py:48-51): the flag filtration is first
+// shrunk by edge collapses, which leave every persistence diagram unchanged.
+// giotto-ph (PyPI giotto-ph, unpinned in the reference's pyproject.toml) is not
+// part of the reference tree; this restates the published criterion (Boissonnat
+// and Pritam, "Edge collapse and persistence of flag complexes", SoCG 2020)
+// rather than that library's code. An edge uv is dominated in a graph when a
+// vertex w adjacent to u and v is adjacent to every other common neighbour of
+// u and v; removing a dominated edge is a strong collapse of the flag complex,
+// so the smaller complex includes into the larger by a homotopy equivalence.
+// Edges are taken from the last to the first. Each is inserted at the first
+// time (original edge index) at which it is not dominated in the graph of that
+// time -- earlier edges at their own times, later ones at the times already
+// chosen -- and dropped if it stays dominated to the end. Each such move keeps
+// the graph of every time the old graph minus an edge dominated in it, so the
+// persistence modules stay isomorphic through the inclusions and the diagrams,
+// read by filtration value, are unchanged. Test infrastructure: it shows that
+// a collapsed and an uncollapsed filtration give the same diagrams.
+//
+// slot[e] = the time from which edge e is present after the collapse (e itself
+// when unchanged), -1 when dropped. Dense n x n table: small inputs only.
+bool collapse_edges(i64 n, const std::vector<i32>& ei, const std::vector<i32>& ej, std::vector<i64>& slot,
+                    i64& removed, i64& delayed) {
+  const i64 E = (i64)ei.size();
+  const i32 NONE = INT32_MAX;
+  if (n > 4096) return false;
+  std::vector<i32> at((size_t)(n * n), NONE);  // at[a * n + b]: time from which edge ab is present
+  for (i64 e = 0; e < E; ++e) at[(size_t)(ei[e] * n + ej[e])] = at[(size_t)(ej[e] * n + ei[e])] = (i32)e;
+  slot.assign(E, 0);
+  removed = delayed = 0;
+  std::vector<i32> times, common;
+  for (i64 k = E - 1; k >= 0; --k) {
+    const i64 u = ei[k], v = ej[k];
+    // the common neighbourhood of u and v changes only when an edge at u or v
+    // appears; between such times a dominating vertex stays dominating (its
+    // own neighbourhood only grows)
+    times.clear();
+    times.push_back((i32)k);
+    for (i64 x = 0; x < n; ++x) {
+      if (x == u || x == v) continue;
+      const i32 a = at[(size_t)(u * n + x)], b = at[(size_t)(v * n + x)];
+      if (a != NONE && a > k) times.push_back(a);
+      if (b != NONE && b > k) times.push_back(b);
+    }
+    std::sort(times.begin(), times.end());
+    times.erase(std::unique(times.begin(), times.end()), times.end());
+    i32 s = NONE;
+    for (i32 t : times) {
+      common.clear();
+      for (i64 x = 0; x < n; ++x)
+        if (x != u && x != v && at[(size_t)(u * n + x)] <= t && at[(size_t)(v * n + x)] <= t) common.push_back((i32)x);
+      bool dom = false;
+      for (i32 w : common) {
+        bool all = true;
+        for (i32 x : common)
+          if (x != w && at[(size_t)(w * n + x)] > t) {
+            all = false;
+            break;
+          }
+        if (all) {
+          dom = true;
+          break;
+        }
+      }
+      if (!dom) {
+        s = t;
+        break;
+      }
+    }
+    if (s == NONE) {
+      slot[k] = -1;
+      at[(size_t)(u * n + v)] = at[(size_t)(v * n + u)] = NONE;
+      ++removed;
+    } else {
+      slot[k] = s;
+      at[(size_t)(u * n + v)] = at[(size_t)(v * n + u)] = s;
+      if (s != k) ++delayed;
+    }
+  }
+  return true;
+}
+
+// H0 and, up to max_dim, H1 and H2 of the sorted filtration in R (edge ranks =
+// filtration order, filt = value per rank): persistence.py:160-215.
+void run_from_sorted(Result* R, i64 n, const std::vector<float>& filt, int max_dim, int stop_after) {
+  const i64 E = (i64)R->edge_i.size();
+  boruvka(R->edge_i, R->edge_j, n, R->mst_idx, R->n_components);
+  std::vector<float> deaths;
+  for (i64 e : R->mst_idx) deaths.push_back(filt[e]);
+  std::sort(deaths.begin(), deaths.end());
+  for (float x : deaths) {
+    R->h0.push_back(0.0f);
+    R->h0.push_back(x);
+  }
+  for (i64 c = 0; c < R->n_components; ++c) {
+    R->h0.push_back(0.0f);
+    R->h0.push_back(INFINITY);
+  }
+  if (stop_after == 2 || max_dim == 0) return;
+  CSR g = vertex_csr(R->edge_i, R->edge_j, n);
+  std::vector<char> mst_mask(E, 0);
+  for (i64 e : R->mst_idx) mst_mask[e] = 1;
+  Triangles tr = enumerate_triangles(R->edge_i, R->edge_j, g);
+  h1_native(*R, n, g, tr, mst_mask, filt);
+  if (max_dim >= 2) h2_blocks(*R, g, tr, filt);
+}
+
 extern "C" {
 
 // Squared threshold as the reference forms it: double product, then FP32
@@ -616,7 +728,6 @@ void* oracle_run(const float* pts, int64_t n, int d, double max_edge_length, int
   sort_edges(R->edge_i, R->edge_j, R->edge_dsq);
   if (stop_after == 1) return R;
   const i64 E = (i64)R->edge_i.size();
-  boruvka(R->edge_i, R->edge_j, n, R->mst_idx, R->n_components);
   std::vector<float> filt(E);
   if (filt_override) {
     if (n_override != E) {
@@ -627,24 +738,51 @@ void* oracle_run(const float* pts, int64_t n, int d, double max_edge_length, int
   } else {
     for (i64 e = 0; e < E; ++e) filt[e] = std::sqrt(R->edge_dsq[e]);
   }
-  std::vector<float> deaths;
-  for (i64 e : R->mst_idx) deaths.push_back(filt[e]);
-  std::sort(deaths.begin(), deaths.end());
-  for (float x : deaths) {
-    R->h0.push_back(0.0f);
-    R->h0.push_back(x);
+  run_from_sorted(R, n, filt, max_dim, stop_after);
+  return R;
+}
+
+// The same filtration after the edge collapse above, then H0..H2 of it (the
+// collapse step giotto-ph takes before its reduction, persistence.py:48-51).
+// Small inputs only (n <= 4096).
+void* oracle_run_collapsed(const float* pts, int64_t n, int d, double max_edge_length, int max_dim,
+                           int fused, int nthreads) {
+  Result* R = new Result();
+  const float thr = oracle_threshold_sq(max_edge_length);
+  if (n <= 1) {
+    if (n == 1) {
+      R->h0 = {0.0f, INFINITY};
+      R->n_components = 1;
+    }
+    return R;
   }
-  for (i64 c = 0; c < R->n_components; ++c) {
-    R->h0.push_back(0.0f);
-    R->h0.push_back(INFINITY);
+  enumerate_edges(pts, n, d, thr, fused, nthreads, R->edge_i, R->edge_j, R->edge_dsq);
+  sort_edges(R->edge_i, R->edge_j, R->edge_dsq);
+  const i64 E = (i64)R->edge_i.size();
+  R->E_full = E;
+  std::vector<i64> slot;
+  if (!collapse_edges(n, R->edge_i, R->edge_j, slot, R->collapse_removed, R->collapse_delayed)) {
+    R->error = "oracle_run_collapsed: n > 4096";
+    return R;
   }
-  if (stop_after == 2 || max_dim == 0) return R;
-  CSR g = vertex_csr(R->edge_i, R->edge_j, n);
-  std::vector<char> mst_mask(E, 0);
-  for (i64 e : R->mst_idx) mst_mask[e] = 1;
-  Triangles tr = enumerate_triangles(R->edge_i, R->edge_j, g);
-  h1_native(*R, n, g, tr, mst_mask, filt);
-  if (max_dim >= 2) h2_blocks(*R, g, tr, filt);
+  std::vector<float> filt0(E);
+  for (i64 e = 0; e < E; ++e) filt0[e] = std::sqrt(R->edge_dsq[e]);
+  std::vector<i64> keep;
+  for (i64 e = 0; e < E; ++e)
+    if (slot[e] >= 0) keep.push_back(e);
+  std::stable_sort(keep.begin(), keep.end(), [&](i64 a, i64 b) { return slot[a] < slot[b]; });
+  std::vector<i32> ni, nj;
+  std::vector<float> nd, filt;
+  for (i64 e : keep) {
+    ni.push_back(R->edge_i[e]);
+    nj.push_back(R->edge_j[e]);
+    nd.push_back(R->edge_dsq[e]);
+    filt.push_back(filt0[slot[e]]);
+  }
+  R->edge_i.swap(ni);
+  R->edge_j.swap(nj);
+  R->edge_dsq.swap(nd);
+  run_from_sorted(R, n, filt, max_dim, 0);
   return R;
 }
 
@@ -701,6 +839,9 @@ int64_t oracle_scalar(void* h, const char* name) {
   if (s == "xor_elems") return R->xor_elems;
   if (s == "crit_path") return R->crit_path;
   if (s == "col_max") return R->col_max;
+  if (s == "E_full") return R->E_full;
+  if (s == "collapse_removed") return R->collapse_removed;
+  if (s == "collapse_delayed") return R->collapse_delayed;
   return -1;
 }
 
