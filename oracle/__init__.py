@@ -20,10 +20,10 @@ _lib = None
 _DT = {1: np.int32, 2: np.int64, 3: np.float32}
 ARRAYS = ("edge_i", "edge_j", "edge_dsq", "mst_idx", "h0", "tri_max_rank_sorted",
           "ap_births", "ap_deaths", "res_births", "res_deaths", "ess_births",
-          "h1_all_pivots", "h1", "h2", "h2_births", "h2_deaths", "h2_ess")
+          "h1_all_pivots", "h1", "h2", "h2_births", "h2_deaths", "h2_ess", "slot_seq", "slot_rounds")
 SCALARS = ("E", "n_components", "T", "Q", "cofacet_nnz", "n_apparent", "residual", "xor_ops",
            "xor_max", "xor_elems", "crit_path", "col_max", "E_full", "collapse_removed",
-           "collapse_delayed")
+           "collapse_delayed", "collapse_rounds")
 
 
 def build(force: bool = False) -> str:
@@ -47,6 +47,9 @@ def _load():
         lib.oracle_run_collapsed.restype = ctypes.c_void_p
         lib.oracle_run_collapsed.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.oracle_collapse_slots.restype = ctypes.c_void_p
+        lib.oracle_collapse_slots.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_int, ctypes.c_int]
         lib.oracle_error.restype = ctypes.c_char_p
         lib.oracle_error.argtypes = [ctypes.c_void_p]
         lib.oracle_free.argtypes = [ctypes.c_void_p]
@@ -104,6 +107,21 @@ def run_collapsed(points, max_edge_length: float, max_dim: int = 2, fused: bool 
     n, d = pts.shape
     h = lib.oracle_run_collapsed(pts.ctypes.data if n else None, n, d, float(max_edge_length),
                                  int(max_dim), int(bool(fused)), int(nthreads))
+    return _collect(lib, h)
+
+
+def collapse_slots(points, max_edge_length: float, fused: bool = True, nthreads: int = 0) -> dict:
+    """The edge collapse's slot per sorted edge computed two ways: last to
+    first (``slot_seq``) and in dependency rounds (``slot_rounds``, with
+    ``collapse_rounds`` rounds). A slot is the edge index from which the edge
+    is present after the collapse, -1 when it is dropped. Small inputs only."""
+    lib = _load()
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+    if pts.ndim != 2:
+        raise ValueError("points must be (n, d)")
+    n, d = pts.shape
+    h = lib.oracle_collapse_slots(pts.ctypes.data if n else None, n, d, float(max_edge_length),
+                                  int(bool(fused)), int(nthreads))
     return _collect(lib, h)
 
 

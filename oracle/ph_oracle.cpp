@@ -50,7 +50,8 @@ struct Result {
   std::vector<i32> h2_births, h2_deaths, h2_ess;
   // edge collapse (oracle_run_collapsed): edges of the full filtration, edges
   // dropped, edges inserted later than their own time
-  i64 E_full = 0, collapse_removed = 0, collapse_delayed = 0;
+  i64 E_full = 0, collapse_removed = 0, collapse_delayed = 0, collapse_rounds = 0;
+  std::vector<i64> slot_seq, slot_rounds;  // oracle_collapse_slots
   std::string error;
 };
 
@@ -672,6 +673,124 @@ bool collapse_edges(i64 n, const std::vector<i32>& ei, const std::vector<i32>& e
   return true;
 }
 
+// The same collapse in rounds, the form a GPU kernel can take: the decision
+// for edge e = uv reads only the edges that share a triangle with it ((u,x) and
+// (v,x) for a common neighbour x) and the edges joining two common neighbours
+// (the dominance certificates), later edges at their final times and earlier
+// ones at their own. A round decides, all at once, every undecided edge whose
+// later such edges are all decided, so each decision sees what the
+// last-to-first order above would show it and the slots come out identical
+// (common neighbours are taken in the full graph, a superset of every time's).
+// rounds = the number of rounds, the length of the longest dependency chain.
+bool collapse_edges_rounds(i64 n, const std::vector<i32>& ei, const std::vector<i32>& ej,
+                           std::vector<i64>& slot, i64& removed, i64& delayed, i64& rounds) {
+  const i64 E = (i64)ei.size();
+  const i64 UNDECIDED = -2, DROPPED = -1;
+  const i64 NONE = INT64_MAX;
+  CSR g = vertex_csr(ei, ej, n);
+  auto edge_id = [&](i32 a, i32 b) -> i64 { return edge_rank_lookup(g, a, b); };
+  slot.assign(E, UNDECIDED);
+  removed = delayed = rounds = 0;
+  // per edge: common neighbours x with the ids of (u,x) and (v,x)
+  auto commons = [&](i64 e, std::vector<i32>& xs, std::vector<i64>& eu, std::vector<i64>& ev) {
+    xs.clear();
+    eu.clear();
+    ev.clear();
+    const i32 u = ei[e], v = ej[e];
+    int p = g.ptr[u], q = g.ptr[v];
+    while (p < g.ptr[u + 1] && q < g.ptr[v + 1]) {
+      if (g.idx[p] < g.idx[q]) ++p;
+      else if (g.idx[p] > g.idx[q]) ++q;
+      else {
+        xs.push_back(g.idx[p]);
+        eu.push_back(g.rank[p]);
+        ev.push_back(g.rank[q]);
+        ++p;
+        ++q;
+      }
+    }
+  };
+  std::vector<i32> xs;
+  std::vector<i64> eu, ev;
+  // the edges whose decision e waits for (later edges of its triangles and certificates)
+  auto waits_on = [&](i64 e, std::vector<i64>& out) {
+    out.clear();
+    commons(e, xs, eu, ev);
+    for (size_t a = 0; a < xs.size(); ++a) {
+      if (eu[a] > e) out.push_back(eu[a]);
+      if (ev[a] > e) out.push_back(ev[a]);
+      for (size_t b = a + 1; b < xs.size(); ++b) {
+        const i64 f = edge_id(xs[a], xs[b]);
+        if (f > e) out.push_back(f);
+      }
+    }
+  };
+  auto decide = [&](i64 e) -> i64 {
+    commons(e, xs, eu, ev);
+    auto time_of = [&](i64 f) -> i64 {  // when edge f is present, as e's decision sees it
+      if (f < 0) return NONE;
+      if (f <= e) return f;
+      return slot[f] == DROPPED ? NONE : (slot[f] == UNDECIDED ? f : slot[f]);
+    };
+    std::vector<i64> tj(xs.size()), times{e};
+    for (size_t a = 0; a < xs.size(); ++a) {
+      const i64 ta = time_of(eu[a]), tb = time_of(ev[a]);
+      tj[a] = (ta == NONE || tb == NONE) ? NONE : std::max(ta, tb);  // x joins the common neighbourhood
+      if (tj[a] != NONE && tj[a] > e) times.push_back(tj[a]);
+    }
+    std::sort(times.begin(), times.end());
+    times.erase(std::unique(times.begin(), times.end()), times.end());
+    std::vector<size_t> C;
+    for (i64 t : times) {
+      C.clear();
+      for (size_t a = 0; a < xs.size(); ++a)
+        if (tj[a] <= t) C.push_back(a);
+      bool dom = false;
+      for (size_t w : C) {
+        bool all = true;
+        for (size_t x : C)
+          if (x != w && time_of(edge_id(xs[w], xs[x])) > t) {
+            all = false;
+            break;
+          }
+        if (all) {
+          dom = true;
+          break;
+        }
+      }
+      if (!dom) return t;
+    }
+    return DROPPED;
+  };
+  std::vector<i64> ready, waits, made;
+  i64 left = E;
+  while (left > 0) {
+    ready.clear();
+    for (i64 e = 0; e < E; ++e) {
+      if (slot[e] != UNDECIDED) continue;
+      waits_on(e, waits);
+      bool ok = true;
+      for (i64 f : waits)
+        if (slot[f] == UNDECIDED) {
+          ok = false;
+          break;
+        }
+      if (ok) ready.push_back(e);
+    }
+    if (ready.empty()) return false;  // cannot happen: the latest undecided edge waits on nothing undecided
+    made.resize(ready.size());
+    for (size_t a = 0; a < ready.size(); ++a) made[a] = decide(ready[a]);
+    for (size_t a = 0; a < ready.size(); ++a) {
+      slot[ready[a]] = made[a];
+      if (made[a] == DROPPED) ++removed;
+      else if (made[a] != ready[a]) ++delayed;
+    }
+    left -= (i64)ready.size();
+    ++rounds;
+  }
+  return true;
+}
+
 // H0 and, up to max_dim, H1 and H2 of the sorted filtration in R (edge ranks =
 // filtration order, filt = value per rank): persistence.py:160-215.
 void run_from_sorted(Result* R, i64 n, const std::vector<float>& filt, int max_dim, int stop_after) {
@@ -786,6 +905,26 @@ void* oracle_run_collapsed(const float* pts, int64_t n, int d, double max_edge_l
   return R;
 }
 
+// Slots of the edge collapse computed both ways (last to first, and in
+// rounds) on the sorted filtration of the points; arrays "slot_seq" and
+// "slot_rounds", scalar "collapse_rounds". Small inputs only (n <= 4096).
+void* oracle_collapse_slots(const float* pts, int64_t n, int d, double max_edge_length, int fused,
+                            int nthreads) {
+  Result* R = new Result();
+  if (n <= 1) return R;
+  enumerate_edges(pts, n, d, oracle_threshold_sq(max_edge_length), fused, nthreads, R->edge_i, R->edge_j,
+                  R->edge_dsq);
+  sort_edges(R->edge_i, R->edge_j, R->edge_dsq);
+  R->E_full = (i64)R->edge_i.size();
+  i64 rm = 0, dl = 0;
+  if (!collapse_edges(n, R->edge_i, R->edge_j, R->slot_seq, rm, dl) ||
+      !collapse_edges_rounds(n, R->edge_i, R->edge_j, R->slot_rounds, R->collapse_removed, R->collapse_delayed,
+                             R->collapse_rounds)) {
+    R->error = "oracle_collapse_slots: n > 4096 or no edge ready";
+  }
+  return R;
+}
+
 void oracle_free(void* h) { delete static_cast<Result*>(h); }
 
 // Returns a pointer to the named array and its element count (0 if empty).
@@ -816,6 +955,8 @@ const void* oracle_get(void* h, const char* name, int64_t* count, int* dtype) {
   ARR("h2_births", h2_births, 1)
   ARR("h2_deaths", h2_deaths, 1)
   ARR("h2_ess", h2_ess, 1)
+  ARR("slot_seq", slot_seq, 2)
+  ARR("slot_rounds", slot_rounds, 2)
 #undef ARR
   *count = -1;
   *dtype = 0;
@@ -842,6 +983,7 @@ int64_t oracle_scalar(void* h, const char* name) {
   if (s == "E_full") return R->E_full;
   if (s == "collapse_removed") return R->collapse_removed;
   if (s == "collapse_delayed") return R->collapse_delayed;
+  if (s == "collapse_rounds") return R->collapse_rounds;
   return -1;
 }
 

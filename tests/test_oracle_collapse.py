@@ -52,3 +52,15 @@ def test_collapse_on_a_tie_heavy_lattice():
     a = oracle.run(g, 1.5, 2)
     b = oracle.run_collapsed(g, 1.5, 2)
     _same_diagrams(a, b)
+
+
+@pytest.mark.parametrize("name", [c for c in golden_cases(max_n=4096) if load_golden(c)[1]["E"] <= 1000])
+def test_collapse_in_dependency_rounds_equals_last_to_first(name):
+    """The round form (every edge whose later triangle and certificate edges are
+    decided is decided at once, as a kernel would) gives the same slot for every
+    edge as the last-to-first order."""
+    z, meta = load_golden(name)
+    r = oracle.collapse_slots(z["points"], float(z["t"]), fused=False)
+    assert np.array_equal(r["slot_seq"], r["slot_rounds"])
+    assert (r["collapse_rounds"] > 0) == (r["E_full"] > 0)
+    assert r["collapse_rounds"] <= max(r["E_full"], 0)
