@@ -46,7 +46,8 @@ def _load():
                                    ctypes.c_int64]
         lib.oracle_run_collapsed.restype = ctypes.c_void_p
         lib.oracle_run_collapsed.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
-                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int]
         lib.oracle_collapse_slots.restype = ctypes.c_void_p
         lib.oracle_collapse_slots.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_int, ctypes.c_int]
@@ -93,20 +94,21 @@ def run(points, max_edge_length: float, max_dim: int = 1, fused: bool = True,
 
 
 def run_collapsed(points, max_edge_length: float, max_dim: int = 2, fused: bool = True,
-                  nthreads: int = 0) -> dict:
+                  nthreads: int = 0, relaxed: bool = False) -> dict:
     """The oracle pipeline on the edge-collapsed flag filtration (the step
     giotto-ph takes before its reduction in the reference's H2 path,
     persistence.py:48-51). Same keys as ``run``; ``edge_i``/``edge_j`` are
     the collapsed filtration's edges, ``E_full`` the uncollapsed edge count,
-    ``collapse_removed``/``collapse_delayed`` what the collapse did. Small
-    inputs only (n <= 4096)."""
+    ``collapse_removed``/``collapse_delayed`` what the collapse did.
+    ``relaxed`` selects the round form with reservations (``collapse_rounds``
+    rounds) instead of the last-to-first order. Small inputs only (n <= 4096)."""
     lib = _load()
     pts = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
     if pts.ndim != 2:
         raise ValueError("points must be (n, d)")
     n, d = pts.shape
     h = lib.oracle_run_collapsed(pts.ctypes.data if n else None, n, d, float(max_edge_length),
-                                 int(max_dim), int(bool(fused)), int(nthreads))
+                                 int(max_dim), int(bool(fused)), int(nthreads), int(bool(relaxed)))
     return _collect(lib, h)
 
 

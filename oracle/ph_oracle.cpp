@@ -791,6 +791,121 @@ bool collapse_edges_rounds(i64 n, const std::vector<i32>& ei, const std::vector<
   return true;
 }
 
+// A relaxed round form for a kernel: every round, each edge finds how far it
+// can be delayed in the current filtration (the first time, from its current
+// one, at which no common neighbour of its ends dominates the others) and the
+// edges that certify it (per interval between changes of the common
+// neighbourhood: the dominating vertex's edges to u and v and to the other
+// common neighbours). Moves whose certificates meet are resolved by
+// deterministic reservations: a move reserves its own edge and its certificate
+// edges with its priority (later current time first, then higher index) and
+// is applied only if it holds every reservation. Applied moves therefore
+// never touch one another's certificates, so each stays a delay of a
+// dominated edge whatever the others do (the other moves only delay edges,
+// which can only shrink the common neighbourhoods), and the rounds repeat
+// until no edge can move. The result differs from the last-to-first order but
+// is again a sequence of valid moves, so the diagrams are unchanged.
+bool collapse_edges_relaxed(i64 n, const std::vector<i32>& ei, const std::vector<i32>& ej,
+                            std::vector<i64>& slot, i64& removed, i64& delayed, i64& rounds) {
+  const i64 E = (i64)ei.size();
+  const i64 NONE = INT64_MAX;
+  CSR g = vertex_csr(ei, ej, n);
+  std::vector<i64> tm(E);
+  std::iota(tm.begin(), tm.end(), (i64)0);
+  struct Move {
+    i64 e, to, prio;
+    std::vector<i64> cert;
+  };
+  std::vector<Move> moves;
+  std::vector<i32> xs;
+  std::vector<i64> eu, ev, tj, times, reserve(E, -1);
+  std::vector<size_t> C;
+  rounds = 0;
+  for (;;) {
+    moves.clear();
+    for (i64 e = 0; e < E; ++e) {
+      if (tm[e] == NONE) continue;
+      const i32 u = ei[e], v = ej[e];
+      xs.clear();
+      eu.clear();
+      ev.clear();
+      for (int p = g.ptr[u], q = g.ptr[v]; p < g.ptr[u + 1] && q < g.ptr[v + 1];) {
+        if (g.idx[p] < g.idx[q]) ++p;
+        else if (g.idx[p] > g.idx[q]) ++q;
+        else {
+          xs.push_back(g.idx[p]);
+          eu.push_back(g.rank[p]);
+          ev.push_back(g.rank[q]);
+          ++p;
+          ++q;
+        }
+      }
+      tj.assign(xs.size(), NONE);
+      times.assign(1, tm[e]);
+      for (size_t a = 0; a < xs.size(); ++a) {
+        if (tm[eu[a]] == NONE || tm[ev[a]] == NONE) continue;
+        tj[a] = std::max(tm[eu[a]], tm[ev[a]]);
+        if (tj[a] > tm[e]) times.push_back(tj[a]);
+      }
+      std::sort(times.begin(), times.end());
+      times.erase(std::unique(times.begin(), times.end()), times.end());
+      Move m{e, NONE, 0, {}};
+      for (i64 t : times) {
+        C.clear();
+        for (size_t a = 0; a < xs.size(); ++a)
+          if (tj[a] <= t) C.push_back(a);
+        long dom = -1;
+        for (size_t w : C) {
+          bool all = true;
+          for (size_t x : C) {
+            if (x == w) continue;
+            const i64 f = edge_rank_lookup(g, xs[w], xs[x]);
+            if (f < 0 || tm[f] > t) {
+              all = false;
+              break;
+            }
+          }
+          if (all) {
+            dom = (long)w;
+            break;
+          }
+        }
+        if (dom < 0) {
+          m.to = t;
+          break;
+        }
+        m.cert.push_back(eu[dom]);
+        m.cert.push_back(ev[dom]);
+        for (size_t x : C)
+          if (x != (size_t)dom) m.cert.push_back(edge_rank_lookup(g, xs[dom], xs[x]));
+      }
+      if (m.to == tm[e]) continue;  // not dominated at its own time
+      m.prio = tm[e] * (E + 1) + e;
+      moves.push_back(std::move(m));
+    }
+    if (moves.empty()) break;
+    ++rounds;
+    std::fill(reserve.begin(), reserve.end(), (i64)-1);
+    for (const Move& m : moves) {
+      reserve[m.e] = std::max(reserve[m.e], m.prio);
+      for (i64 f : m.cert) reserve[f] = std::max(reserve[f], m.prio);
+    }
+    for (const Move& m : moves) {
+      bool held = reserve[m.e] == m.prio;
+      for (i64 f : m.cert) held = held && reserve[f] == m.prio;
+      if (held) tm[m.e] = m.to;
+    }
+  }
+  slot.resize(E);
+  removed = delayed = 0;
+  for (i64 e = 0; e < E; ++e) {
+    slot[e] = tm[e] == NONE ? -1 : tm[e];
+    if (tm[e] == NONE) ++removed;
+    else if (tm[e] != e) ++delayed;
+  }
+  return true;
+}
+
 // H0 and, up to max_dim, H1 and H2 of the sorted filtration in R (edge ranks =
 // filtration order, filt = value per rank): persistence.py:160-215.
 void run_from_sorted(Result* R, i64 n, const std::vector<float>& filt, int max_dim, int stop_after) {
@@ -861,11 +976,12 @@ void* oracle_run(const float* pts, int64_t n, int d, double max_edge_length, int
   return R;
 }
 
-// The same filtration after the edge collapse above, then H0..H2 of it (the
-// collapse step giotto-ph takes before its reduction, persistence.py:48-51).
-// Small inputs only (n <= 4096).
+// The same filtration after the edge collapse above (relaxed = 0: last to
+// first; 1: the relaxed round form), then H0..H2 of it (the collapse step
+// giotto-ph takes before its reduction, persistence.py:48-51). Small inputs
+// only (n <= 4096).
 void* oracle_run_collapsed(const float* pts, int64_t n, int d, double max_edge_length, int max_dim,
-                           int fused, int nthreads) {
+                           int fused, int nthreads, int relaxed) {
   Result* R = new Result();
   const float thr = oracle_threshold_sq(max_edge_length);
   if (n <= 1) {
@@ -880,7 +996,10 @@ void* oracle_run_collapsed(const float* pts, int64_t n, int d, double max_edge_l
   const i64 E = (i64)R->edge_i.size();
   R->E_full = E;
   std::vector<i64> slot;
-  if (!collapse_edges(n, R->edge_i, R->edge_j, slot, R->collapse_removed, R->collapse_delayed)) {
+  const bool ok = relaxed ? collapse_edges_relaxed(n, R->edge_i, R->edge_j, slot, R->collapse_removed,
+                                                   R->collapse_delayed, R->collapse_rounds)
+                          : collapse_edges(n, R->edge_i, R->edge_j, slot, R->collapse_removed, R->collapse_delayed);
+  if (!ok) {
     R->error = "oracle_run_collapsed: n > 4096";
     return R;
   }

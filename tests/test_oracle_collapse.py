@@ -64,3 +64,17 @@ def test_collapse_in_dependency_rounds_equals_last_to_first(name):
     assert np.array_equal(r["slot_seq"], r["slot_rounds"])
     assert (r["collapse_rounds"] > 0) == (r["E_full"] > 0)
     assert r["collapse_rounds"] <= max(r["E_full"], 0)
+
+
+@pytest.mark.parametrize("name", [c for c in golden_cases(max_n=4096) if load_golden(c)[1]["E"] <= 1500])
+def test_relaxed_round_collapse_keeps_every_diagram(name):
+    """The relaxed round form (moves resolved by reservations, repeated until
+    no edge can move) ends elsewhere than the last-to-first order but is a
+    sequence of valid moves too: the same diagrams, at least as many edges
+    removed on these fixtures."""
+    z, meta = load_golden(name)
+    a = oracle.run(z["points"], float(z["t"]), meta["max_dim"], fused=False)
+    b = oracle.run_collapsed(z["points"], float(z["t"]), meta["max_dim"], fused=False)
+    c = oracle.run_collapsed(z["points"], float(z["t"]), meta["max_dim"], fused=False, relaxed=True)
+    _same_diagrams(a, c)
+    assert c["E"] <= b["E"]
