@@ -66,7 +66,12 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms.
+
+    Entering waits (up to 3 s) until nvidia-smi has produced its first sample,
+    so that sampling is live when the timed region starts; the summary then
+    uses the samples taken inside the region, or every sample when the region
+    was too short to see one."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -85,8 +90,12 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.monotonic()
+            while not self.lines and self.proc.poll() is None and time.monotonic() - t0 < 3.0:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
+        self.first = len(self.lines)
         return self
 
     def _read(self):
@@ -102,9 +111,16 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        inside = self._summary(self.lines[self.first:])
+        if inside["samples"]:
+            return dict(inside, in_region=True)
+        return dict(self._summary(self.lines), in_region=False)
+
+    @staticmethod
+    def _summary(lines):
         sm, mx, reasons = [], None, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
+        for ln in lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -614,7 +630,9 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 300 for the plain workload, so that the clock sampler sees "
+                         "the timed region; 20 otherwise)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("flashph", "reference"), default="flashph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -627,6 +645,8 @@ def main():
     ap.add_argument("--t", type=float, default=None, help="precision workload: max_edge_length")
     ap.add_argument("--max-dim", type=int, default=None, help="precision workload: max_dim")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 300 if args.impl == "flashph" and args.workload == "plain" else 20
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
