@@ -35,7 +35,8 @@ extern "C" {
 #define PH_ERR_OVERFLOW 6    /* a count does not fit the index type          */
 #define PH_ERR_LIMIT 7       /* a user limit was exceeded (ValueError text)  */
 
-/* Library version (major*10000 + minor*100 + patch). */
+/* Library version (major*10000 + minor*100 + patch). No counterpart in the
+ * reference (library utility), like the two functions below. */
 int ph_version(void);
 
 /* Last CUDA error string seen by the library on this thread ("" if none). */
@@ -80,17 +81,22 @@ int ph_edges_enumerate(const float* pts, int64_t n, int32_t d, float thr_sq, int
                        int32_t* out_j, float* out_dsq, int64_t capacity,
                        unsigned long long* d_count, void* stream);
 
-/* Edge-enumeration work items (128 x 128 point tiles) of a cloud of n points. */
+/* Edge-enumeration work items (128 x 128 point tiles, i-tile <= j-tile) of a
+ * cloud of n points: the counterpart of the reference kernel's program grid
+ * (kernels/edge_kernel.py:208-210, 32-point tiles). */
 int64_t ph_cloud_tiles(int64_t n);
 
 /* ph_edges_enumerate over a batch: segs (device) holds nsegs clouds ordered
  * by tile_off; ntiles is the total number of work items. Vertex indices
- * are written as global indices. */
+ * are written as global indices. Replaces one kernels/edge_kernel.py:152
+ * direct_edge_enumerate call per cloud (rips.py:151-159); the reference has
+ * no batched form. */
 int ph_batch_edges_enumerate(const float* pts, const ph_cloud_seg* segs, int32_t nsegs, int64_t ntiles,
                              int32_t* out_i, int32_t* out_j, float* out_dsq, int64_t capacity,
                              unsigned long long* d_count, void* stream);
 
-/* ph_batch_edges_enumerate with a tensor-core screen (d <= 252): every
+/* ph_batch_edges_enumerate with a tensor-core screen (d <= 252), also
+ * replacing kernels/edge_kernel.py:152 direct_edge_enumerate: every
  * cloud is centred on its mean and rounded to BF16, 128 x 128 point tiles
  * of an augmented Gram matrix (|y_i|^2 + |y_j|^2 - 2 y_i.y_j) are formed by
  * tcgen05.mma into tensor memory, and each value is compared with the
@@ -199,7 +205,9 @@ int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx, int64_t n
                        unsigned long long* d_total, int* d_next, void* stream);
 
 /* Writes, for every triangle in global order, its largest edge tri_m, third
- * vertex tri_w and the ranks of its two other edges (a,w) and (b,w). */
+ * vertex tri_w and the ranks of its two other edges (a,w) and (b,w): the emit
+ * pass of triangle_kernel.py:288 triangle_enumerate with the face ranks of
+ * reduce_h1_gpu.py:65-100. */
 int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
                       const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
                       const int64_t* tri_off, int32_t* tri_m, int32_t* tri_w, int32_t* tri_fa,
@@ -221,7 +229,9 @@ int ph_tets_count(const int64_t* tri_off, const int32_t* tri_w, int64_t E,
                   size_t workspace_bytes, void* stream);
 
 /* Writes per tetrahedron its largest edge and the local indices (triangle
- * global rank - E) of its four triangle faces. tet_faces: Q x 4.
+ * global rank - E) of its four triangle faces (the emit kernel of
+ * triangle_kernel.py:402 tetrahedra_enumerate with the face lookup of
+ * apparent_pair_h2_kernel.py:37-49). tet_faces: Q x 4.
  * d_status gets PH_ERR_ARG if a face triangle cannot be found (inconsistent
  * inputs). */
 int ph_tets_emit(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int64_t* tri_off,
@@ -309,7 +319,9 @@ typedef struct ph_result ph_result;
 int ph_rips_persistence(const float* points, int64_t n, int32_t d, double max_edge_length, int32_t max_dim,
                         int64_t max_triangles, int64_t max_tetrahedra, int32_t edge_mode, ph_result** out,
                         void* stream);
-/* rows of diagram dim (0..max_dim), -1 if out of range */
+/* Accessors of ph_rips_persistence's result, the list of (K, 2) diagrams
+ * that persistence.py:77 returns.
+ * rows of diagram dim (0..max_dim), -1 if out of range */
 int64_t ph_result_rows(const ph_result* result, int32_t dim);
 /* run statistics: 0 edges, 1 triangles, 2 tetrahedra, 3 H1 column additions,
  * 4 H2 column additions */
@@ -323,8 +335,11 @@ int ph_result_copy_all(const ph_result* result, float* dst, int32_t to_host, voi
 void ph_result_free(ph_result* result);
 
 /* ---- batches of clouds ---------------------------------------------------- */
+/* The reference has no batched API; each entry below does, for every cloud of
+ * a batch at once, what the cited per-cloud step does for one cloud. */
 
-/* vcloud[v] = cloud of global vertex v (N = sum of n over the batch). */
+/* vcloud[v] = cloud of global vertex v (N = sum of n over the batch); batch
+ * bookkeeping with no per-cloud counterpart. */
 int ph_batch_vertex_cloud(const ph_cloud_seg* segs, int32_t nsegs, int32_t* vcloud, void* stream);
 
 /* Per-cloud filtration order of a batch's edges: each cloud's edges sorted
@@ -338,7 +353,8 @@ int ph_batch_edges_sort(const int32_t* in_i, const int32_t* in_j, const float* i
                         size_t workspace_bytes, void* stream);
 
 /* off[c] = first item of cloud c for items grouped by cloud, identified by
- * one vertex each (item_vertex); off[nsegs] = n_items. */
+ * one vertex each (item_vertex); off[nsegs] = n_items. Batch bookkeeping
+ * with no per-cloud counterpart. */
 int ph_batch_item_offsets(const int32_t* item_vertex, int64_t n_items, const int32_t* vcloud, int32_t nsegs,
                           int64_t* off, void* stream);
 
@@ -349,29 +365,33 @@ int ph_batch_h0_rows(const float* edge_filt, const uint8_t* mst_mask, int64_t E,
                      const ph_cloud_seg* segs, int32_t nsegs, const int32_t* vcloud, int64_t N,
                      float* out_rows, void* workspace, size_t workspace_bytes, void* stream);
 
-/* ph_persistence_rows per cloud: col_off (nsegs+1) are the per-cloud column
- * offsets; row_off (nsegs+1) receives the per-cloud row offsets. */
+/* ph_persistence_rows per cloud (reduce_h1_gpu.py:574-604 per cloud):
+ * col_off (nsegs+1) are the per-cloud column offsets; row_off (nsegs+1)
+ * receives the per-cloud row offsets. */
 size_t ph_batch_persistence_rows_workspace_bytes(int64_t K);
 int ph_batch_persistence_rows(const int32_t* col_state, const int32_t* col_piv, int64_t K, int32_t row_base,
                               const float* filt, const int32_t* col_m, const int32_t* row_m,
                               const int64_t* col_off, int32_t nsegs, float* out_rows, int64_t* row_off,
                               int64_t* d_nrows, void* workspace, size_t workspace_bytes, void* stream);
 
-/* out[e] = 1 if edge e's cloud has max_dim >= min_dim. */
+/* out[e] = 1 if edge e's cloud has max_dim >= min_dim: the per-cloud
+ * max_dim branch of persistence.py:185-215 as an edge mask. */
 int ph_batch_edge_dim_mask(const int32_t* edge_i, int64_t E, const int32_t* vcloud, const ph_cloud_seg* segs,
                            int32_t min_dim, uint8_t* out, void* stream);
 
-/* dst[i] |= src[idx[i]] (or its negation when invert != 0). */
+/* dst[i] |= src[idx[i]] (or its negation when invert != 0); mask plumbing
+ * for the batch, no per-cloud counterpart. */
 int ph_or_gather_mask(uint8_t* dst, const uint8_t* src, const int32_t* idx, int64_t n, int32_t invert,
                       void* stream);
 
 /* k-th nearest-neighbour distance of every point of every cloud, k clamped
- * to n_c - 1 per cloud. qb_off (nsegs+1): per-cloud offsets of 128-point
+ * to n_c - 1 per cloud (threshold.py:133-176 _tiled_knn per cloud). qb_off (nsegs+1): per-cloud offsets of 128-point
  * query blocks; nqb their total; max_d the largest d. out: N floats. */
 int ph_batch_knn_kth(const float* pts, const ph_cloud_seg* segs, int32_t nsegs, const int64_t* qb_off,
                      int64_t nqb, int32_t max_d, int32_t k, float* out, void* stream);
 
-/* torch.quantile semantics per cloud over values[vbase_c .. vbase_c+n_c). */
+/* torch.quantile semantics per cloud over values[vbase_c .. vbase_c+n_c)
+ * (the quantile of threshold.py:77 per cloud). */
 size_t ph_batch_quantile_workspace_bytes(int64_t N);
 int ph_batch_quantile(const float* values, int64_t N, const int32_t* vcloud, const ph_cloud_seg* segs,
                       int32_t nsegs, double q, float* out, void* workspace, size_t workspace_bytes,
