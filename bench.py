@@ -65,27 +65,102 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
+def gpu_selector(local: int) -> str:
+    """The nvidia-smi / NVML identifier of torch device ``local``.
+
+    nvidia-smi and NVML number the physical GPUs and ignore
+    CUDA_VISIBLE_DEVICES, so a job given, say, physical GPU 5 as cuda:0 must
+    name its GPU by UUID, or it reads another GPU's clocks."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(local).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:  # no CUDA (CPU tests): the index is all there is
+        return str(local)
+
+
+class NvmlClockPoller:
+    """SM clock and clock-event reasons of one GPU read through NVML every
+    ``period`` seconds from a host thread, so that a timed region of a few
+    milliseconds still holds samples (nvidia-smi samples every 200 ms at
+    best). Inactive (no samples) where NVML cannot be loaded."""
+
+    BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
+
+    def __init__(self, selector: str, period: float = 0.002):
+        self.selector = selector
+        self.period = period
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._nv = None
+
+    def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = (nv.nvmlDeviceGetHandleByUUID(self.selector) if self.selector.startswith("GPU-")
+                 else nv.nvmlDeviceGetHandleByIndex(int(self.selector)))
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._nv, self._h = nv, h
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._nv = None
+        return self
+
+    def _run(self):
+        nv, h = self._nv, self._h
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                     int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+            except Exception:
+                return
+            time.sleep(self.period)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._nv is not None:
+            self._t.join(timeout=2)
+            try:
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
+
+    def summary(self):
+        sm = [s for s, _ in self.samples]
+        reasons = sorted({nm for _, r in self.samples for nm, b in self.BITS.items() if r & b})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sm)}
+
+
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms.
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms, plus NVML
+    samples every 2 ms, of the GPU named by ``selector`` (its UUID; a
+    bare index only where no UUID is known).
 
     Entering waits (up to 3 s) until nvidia-smi has produced its first sample,
-    so that sampling is live when the timed region starts; the summary then
-    uses the samples taken inside the region, or every sample when the region
-    was too short to see one."""
+    so that sampling is live when the timed region starts. The summary is the
+    NVML samples when there are any (they fall inside the region), else the
+    nvidia-smi samples taken inside the region, else every nvidia-smi sample
+    when the region was too short to see one; ``smi`` always carries the
+    nvidia-smi summary."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
-        self.index = index
+    def __init__(self, selector):
+        self.selector = str(selector)
         self.proc = None
         self.lines: list[str] = []
+        self.nvml = NvmlClockPoller(self.selector)
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", "-i", self.selector, f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -96,6 +171,7 @@ class ClockSampler:
         except OSError:
             self.proc = None
         self.first = len(self.lines)
+        self.nvml.__enter__()
         return self
 
     def _read(self):
@@ -103,6 +179,7 @@ class ClockSampler:
             self.lines.append(ln.strip())
 
     def __exit__(self, *a):
+        self.nvml.__exit__(*a)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -110,11 +187,25 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def smi_summary(self):
         inside = self._summary(self.lines[self.first:])
         if inside["samples"]:
             return dict(inside, in_region=True)
         return dict(self._summary(self.lines), in_region=False)
+
+    def summary(self):
+        smi = self.smi_summary()
+        nv = self.nvml.summary()
+        if nv["samples"]:
+            out = dict(nv, in_region=True, source="nvml, 2 ms period, inside the timed region")
+            out["reasons"] = sorted(set(out["reasons"]) | (set(smi["reasons"]) if smi["in_region"] else set()))
+            if out["sm_max_mhz"] is None:
+                out["sm_max_mhz"] = smi["sm_max_mhz"]
+        else:
+            out = dict(smi, source="nvidia-smi, 200 ms period")
+        out["gpu"] = self.selector
+        out["smi"] = smi
+        return out
 
     @staticmethod
     def _summary(lines):
@@ -405,7 +496,7 @@ def run_precision(args, rank, local):
         rips_persistence(pts, t, max_dim=md)
     torch.cuda.synchronize()
     l0 = _lib.launch_count()
-    with ClockSampler(local) as clocks, _timing.record() as stages:
+    with ClockSampler(gpu_selector(local)) as clocks, _timing.record() as stages:
         ms, out = timed(lambda: rips_persistence(pts, t, max_dim=md), steps)
     launches = (_lib.launch_count() - l0) // (steps + 1)
     e2e_ms, res = timed(lambda: rips_persistence(pinned, t, max_dim=md), max(3, steps // 2))
@@ -693,7 +784,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     l0 = _lib.launch_count()
-    with ClockSampler(local) as clocks, _timing.record() as stages:
+    with ClockSampler(gpu_selector(local)) as clocks, _timing.record() as stages:
         for k in range(args.steps):
             flush.zero_()
             starts[k].record()
@@ -758,7 +849,8 @@ def main():
             "roofline": dict(rl.get(dominant, rl["edges"]), stage=dominant),
             "rooflines": rl,
             "cpu_baseline": cpu,
-            "clocks": cs,
+            # device time x median SM clock: thousands of SM cycles per step
+            "clocks": dict(cs, kcycles_per_step=round(ms * cs["sm_mhz"], 1)) if cs.get("sm_mhz") else cs,
             "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
             "stages_source": "staged pipeline (the same stages called one by one from Python), CUDA events "
                              "around each stage, 3 calls outside the timed region; the timed calls run the "

@@ -264,60 +264,7 @@ __global__ void k_or_gather(uint8_t* __restrict__ dst, const uint8_t* __restrict
   }
 }
 
-// ---- thresholds per cloud ----------------------------------------------------------
-constexpr int KN_NT = 128;
-constexpr int KN_TP = 64;
-constexpr int KN_MAXK = 64;
-
-__global__ void __launch_bounds__(KN_NT) k_knn_batch(const float* __restrict__ pts_all,
-                                                    const ph_cloud_seg* __restrict__ segs, int nsegs,
-                                                    const i64* __restrict__ qb_off, int kreq,
-                                                    float* __restrict__ out) {
-  ph::pdl_wait();
-  ph::pdl_trigger();
-  extern __shared__ float sm[];
-  const int c = seg_of(qb_off, nsegs, (i64)blockIdx.x);
-  const ph_cloud_seg sg = segs[c];
-  const float* pts = pts_all + sg.pt_off;
-  const i64 n = sg.n;
-  const int d = sg.d;
-  const int k = (int)min((i64)kreq, n - 1);
-  float* q = sm;
-  float* tile = sm + d * KN_NT;
-  const i64 qi = ((i64)blockIdx.x - qb_off[c]) * KN_NT + threadIdx.x;
-  for (int idx = threadIdx.x; idx < d * KN_NT; idx += KN_NT) {
-    const int t = idx / d, kk = idx - t * d;
-    const i64 g = ((i64)blockIdx.x - qb_off[c]) * KN_NT + t;
-    q[kk * KN_NT + t] = g < n ? pts[g * d + kk] : 0.0f;
-  }
-  float best[KN_MAXK];
-  for (int z = 0; z < KN_MAXK; ++z) best[z] = __int_as_float(0x7f800000);
-  for (i64 j0 = 0; j0 < n; j0 += KN_TP) {
-    __syncthreads();
-    const int tp = (int)((n - j0) < (i64)KN_TP ? (n - j0) : (i64)KN_TP);
-    for (int idx = threadIdx.x; idx < tp * d; idx += KN_NT) tile[idx] = pts[j0 * d + idx];
-    __syncthreads();
-    if (qi >= n || k < 1) continue;
-    for (int jj = 0; jj < tp; ++jj) {
-      const i64 j = j0 + jj;
-      float acc = 0.0f;
-      for (int kk = 0; kk < d; ++kk) {
-        const float df = __fsub_rn(q[kk * KN_NT + threadIdx.x], tile[jj * d + kk]);
-        acc = __fmaf_rn(df, df, acc);
-      }
-      if (j != qi && acc < best[k - 1]) {
-        int z = k - 1;
-        while (z > 0 && best[z - 1] > acc) {
-          best[z] = best[z - 1];
-          --z;
-        }
-        best[z] = acc;
-      }
-    }
-  }
-  if (qi < n) out[sg.vbase + qi] = k >= 1 ? __fsqrt_rn(best[k - 1]) : 0.0f;
-}
-
+// ---- thresholds per cloud (the k-NN scan is in threshold.cu) ----------------------------
 __global__ void k_seg_value_keys(const float* __restrict__ v, i64 N, const i32* __restrict__ vcloud,
                                  u64* __restrict__ keys, u32* __restrict__ vals) {
   ph::pdl_wait();
@@ -503,19 +450,6 @@ extern "C" int ph_or_gather_mask(uint8_t* dst, const uint8_t* src, const int32_t
   if (n == 0) return PH_OK;
   ph::count_launch();
   ph::launch_pdl(k_or_gather, dim3(grid_for(n)), dim3(256), 0, (cudaStream_t)stream, dst, src, idx, n, invert);
-  PH_CHECK_LAUNCH();
-  return PH_OK;
-}
-
-extern "C" int ph_batch_knn_kth(const float* pts, const ph_cloud_seg* segs, int32_t nsegs, const int64_t* qb_off,
-                                int64_t nqb, int32_t max_d, int32_t k, float* out, void* stream) {
-  if (nsegs < 1 || nqb < 0 || max_d < 1 || k < 1 || k > KN_MAXK) return PH_ERR_ARG;
-  if (nqb == 0) return PH_OK;
-  const size_t smem = sizeof(float) * ((size_t)max_d * KN_NT + (size_t)KN_TP * max_d);
-  if (smem > 200 * 1024) return PH_ERR_ARG;
-  if (smem > 48 * 1024) ph::allow_dynamic_smem((const void*)k_knn_batch);
-  ph::count_launch();
-  ph::launch_pdl(k_knn_batch, dim3((unsigned)nqb), dim3(KN_NT), smem, (cudaStream_t)stream, pts, segs, nsegs, qb_off, k, out);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

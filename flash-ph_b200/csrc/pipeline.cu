@@ -325,6 +325,15 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     snprintf(m, sizeof m, "Edge count %lld exceeds int32 range; reduce max_edge_length", (long long)E);
     return give_up(fail(PH_ERR_LIMIT, m));
   }
+  // the second pass ran with a buffer of the first pass's exact count; a
+  // larger count now means the passes disagree, and the buffers hold only cap
+  // edges, so nothing after this may read E of them
+  if (E > cap) {
+    char m[160];
+    snprintf(m, sizeof m, "edge enumeration: %lld edges counted, buffer sized for %lld", (long long)E,
+             (long long)cap);
+    return give_up(fail(PH_ERR_CAPACITY, m));
+  }
   res->stats[0] = E;
 
   // ---- 2. filtration order, adjacency, values ---------------------------------------------
@@ -544,6 +553,28 @@ extern "C" int64_t ph_result_stat(const ph_result* r, int32_t k) {
   return r->stats[k];
 }
 
+namespace {
+// A copy queued on another stream than the run's: the run's stream waits for
+// it, so that ph_result_free's stream-ordered frees cannot overtake it. (The
+// rows themselves are complete when ph_rips_persistence returns: its last
+// host wait follows them in stream order.)
+int order_frees_after(const ph_result* r, cudaStream_t s) {
+  if (s == r->stream) return PH_OK;
+  cudaEvent_t ev;
+  cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) {
+    e = cudaEventRecord(ev, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(r->stream, ev, 0);
+    cudaEventDestroy(ev);
+  }
+  if (e != cudaSuccess) {
+    record_error(e);
+    return PH_ERR_CUDA;
+  }
+  return PH_OK;
+}
+}  // namespace
+
 extern "C" int ph_result_copy(const ph_result* r, int32_t dim, float* dst, int32_t to_host, void* stream) {
   if (!r || dim < 0 || dim >= r->ndim || (!dst && r->nrows[dim])) return PH_ERR_ARG;
   if (!r->nrows[dim]) return PH_OK;
@@ -554,7 +585,7 @@ extern "C" int ph_result_copy(const ph_result* r, int32_t dim, float* dst, int32
     record_error(e);
     return PH_ERR_CUDA;
   }
-  return PH_OK;
+  return order_frees_after(r, (cudaStream_t)stream);
 }
 
 extern "C" int ph_result_copy_all(const ph_result* r, float* dst, int32_t to_host, void* stream) {
@@ -573,7 +604,7 @@ extern "C" int ph_result_copy_all(const ph_result* r, float* dst, int32_t to_hos
     }
     at += r->nrows[k];
   }
-  return PH_OK;
+  return at ? order_frees_after(r, (cudaStream_t)stream) : PH_OK;
 }
 
 extern "C" void ph_result_free(ph_result* r) {

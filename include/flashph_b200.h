@@ -326,12 +326,16 @@ int64_t ph_result_rows(const ph_result* result, int32_t dim);
 /* run statistics: 0 edges, 1 triangles, 2 tetrahedra, 3 H1 column additions,
  * 4 H2 column additions */
 int64_t ph_result_stat(const ph_result* result, int32_t k);
-/* copies diagram dim (rows x 2 float32) to dst, device or host memory */
+/* copies diagram dim (rows x 2 float32) to dst, device or host memory, on
+ * `stream` (any stream: when it is not the run's stream, the run's stream is
+ * made to wait for the copy, so that ph_result_free cannot release the rows
+ * before the copy has read them) */
 int ph_result_copy(const ph_result* result, int32_t dim, float* dst, int32_t to_host, void* stream);
-/* copies every diagram, dim 0 first, into one buffer of sum(rows) x 2 float32 */
+/* copies every diagram, dim 0 first, into one buffer of sum(rows) x 2 float32
+ * (stream rule of ph_result_copy) */
 int ph_result_copy_all(const ph_result* result, float* dst, int32_t to_host, void* stream);
 /* releases the diagrams and the run's intermediate buffers (stream-ordered, on
- * the stream of the run; call it after the copies are queued) */
+ * the stream of the run, after every copy queued before it) */
 void ph_result_free(ph_result* result);
 
 /* ---- batches of clouds ---------------------------------------------------- */

@@ -151,3 +151,55 @@ def _collect(lib, h) -> dict:
     finally:
         lib.oracle_free(h)
     return out
+
+
+# ---- thresholds (threshold.py:20-200), in FP64 ---------------------------------------
+def _sq_dists_f64(q, pts, qn, pn):
+    """Squared distances of rows q to all pts in FP64 by the Gram expansion
+    (relative error ~1e-15 of |x|^2, far below the fp32 values compared
+    against it), clamped at 0."""
+    return np.maximum(qn[:, None] + pn[None, :] - 2.0 * (q @ pts.T), 0.0)
+
+
+def knn_kth_f64(points, k: int, chunk: int = 1024) -> np.ndarray:
+    """k-th nearest-neighbour distance of every point (the point itself
+    excluded, duplicates of it counted at distance 0), in FP64: the quantity
+    ``_tiled_knn`` (threshold.py:133-176) computes with fp32 cdist tiles."""
+    pts = np.asarray(points, dtype=np.float64)
+    n = pts.shape[0]
+    nrm = (pts * pts).sum(1)
+    out = np.empty(n, dtype=np.float64)
+    for s in range(0, n, chunk):
+        q = pts[s:s + chunk]
+        d2 = _sq_dists_f64(q, pts, nrm[s:s + chunk], nrm)
+        d2[np.arange(q.shape[0]), np.arange(s, s + q.shape[0])] = np.inf
+        out[s:s + chunk] = np.sqrt(np.partition(d2, k - 1, axis=1)[:, k - 1])
+    return out
+
+
+def auto_threshold_f64(points, k: int = 20, percentile: float = 95.0) -> float:
+    """auto_threshold (threshold.py:20-78) without subsampling, in FP64: k
+    clamped to [1, n - 1], percentile to [0, 100], linear-interpolation
+    percentile of the k-th NN distances."""
+    pts = np.asarray(points, dtype=np.float64)
+    n = pts.shape[0]
+    if n <= 1:
+        return 0.0
+    k = max(1, min(k, n - 1))
+    percentile = max(0.0, min(100.0, percentile))
+    return float(np.quantile(knn_kth_f64(pts, k), percentile / 100.0, method="linear"))
+
+
+def enclosing_radius_f64(points, chunk: int = 1024) -> float:
+    """enclosing_radius (threshold.py:81-116, 179-200) without subsampling,
+    in FP64: min over points of the max distance to any point."""
+    pts = np.asarray(points, dtype=np.float64)
+    n = pts.shape[0]
+    if n <= 1:
+        return 0.0
+    nrm = (pts * pts).sum(1)
+    best = np.inf
+    for s in range(0, n, chunk):
+        d2 = _sq_dists_f64(pts[s:s + chunk], pts, nrm[s:s + chunk], nrm)
+        best = min(best, float(np.sqrt(d2.max(axis=1)).min()))
+    return best

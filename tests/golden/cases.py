@@ -122,3 +122,26 @@ CASES = [
 ]
 
 CASE_BY_NAME = {c["name"]: c for c in CASES}
+
+
+def _th(name, gen, n, d, k=20, percentile=95.0, seed=42, **args):
+    return {"name": name, "gen": gen, "n": n, "d": d, "t": 0.0, "max_dim": 0, "seed": seed, "args": args,
+            "k": k, "percentile": percentile}
+
+
+# auto_threshold / enclosing_radius cases (threshold.py:20-200): the defaults
+# (k=20, 95th percentile), the larger k the reference's docstring recommends
+# for tori (k >= 50), k above 64 and d far above the edge kernels' range,
+# exact ties on a lattice, and k clamped to n - 1.
+THRESH_CASES = [
+    _th("th_n500_d10", "gaussian", 500, 10),
+    _th("th_n2000_d3", "gaussian", 2000, 3),
+    _th("th_n300_d50_k5_p50", "gaussian", 300, 50, k=5, percentile=50.0),
+    _th("th_clifford400_k50", "clifford", 400, 4, k=50, noise=0.02),
+    _th("th_n1000_d512_k100_p90", "gaussian", 1000, 512, k=100, percentile=90.0, seed=7),
+    _th("th_n700_d300_k64_p99", "gaussian", 700, 300, k=64, percentile=99.0, seed=8),
+    _th("th_n1500_d8_k200", "gaussian", 1500, 8, k=200, percentile=95.0, seed=9),
+    _th("th_grid3_k6_p50", "grid3", 27, 3, k=6, percentile=50.0),
+    _th("th_n50_d2_k100", "gaussian", 50, 2, k=100, percentile=75.0, seed=11),
+    _th("th_n2_d3", "gaussian", 2, 3, k=20, seed=12),
+]

@@ -1,10 +1,13 @@
 """Generate golden fixtures by running the reference implementation on the CPU.
 
 This script is test infrastructure. It imports the reference package
-(ot-triton-lab/flash-ph) from ``/root/reference/src`` and runs its own code
-on seeded inputs, writing one ``.npz`` per case into this directory plus
-``manifest.json``. The GPU box never runs it; the committed fixtures travel
-instead.
+(ot-triton-lab/flash-ph) from the ``src`` directory of a checkout, named with
+``--reference PATH`` or the ``FLASHPH_REFERENCE_SRC`` environment variable,
+and runs its own code on seeded inputs, writing one ``.npz`` per case into
+this directory plus ``manifest.json``, and the reference's ``auto_threshold``
+and ``enclosing_radius`` values for the threshold cases into
+``thresholds.json``. The GPU box never runs it; the committed fixtures
+travel instead.
 
 How the reference is driven (all of it is the reference's own code):
 
@@ -29,7 +32,12 @@ How the reference is driven (all of it is the reference's own code):
   MST edges skipped, then H2 with the H1 pivots cleared). The H1 diagram of
   that assembly is checked to equal the native H1 diagram as a multiset.
 
-Run: ``python tests/golden/make_golden.py`` (takes a few minutes).
+* Thresholds: ``threshold.py:20 auto_threshold`` and ``threshold.py:81
+  enclosing_radius`` called on numpy inputs (CPU tensors, fp32 ``cdist``
+  tiles), without subsampling.
+
+Run: ``python tests/golden/make_golden.py --reference <checkout>/src [case ...]``
+(takes a few minutes); ``--thresholds`` writes only ``thresholds.json``.
 """
 from __future__ import annotations
 
@@ -41,17 +49,30 @@ import time
 os.environ.setdefault("TRITON_INTERPRET", "1")
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/flashph_numba_cache")
 
-REF_SRC = "/root/reference/src"
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
-from cases import CASES, make_points  # noqa: E402
+from cases import CASES, THRESH_CASES, make_points  # noqa: E402
 
 
-def _load_reference():
-    sys.path.insert(0, REF_SRC)
+def _reference_src(argv: list[str]) -> str:
+    """The reference checkout's ``src`` directory: ``--reference PATH`` or
+    ``FLASHPH_REFERENCE_SRC``."""
+    if "--reference" in argv:
+        k = argv.index("--reference")
+        path = argv[k + 1]
+        del argv[k:k + 2]
+    else:
+        path = os.environ.get("FLASHPH_REFERENCE_SRC", "")
+    if not path or not os.path.isdir(os.path.join(path, "flash_ph")):
+        raise SystemExit("name the reference's src directory with --reference PATH or FLASHPH_REFERENCE_SRC")
+    return path
+
+
+def _load_reference(src: str):
+    sys.path.insert(0, src)
     from flash_ph import rips
     from flash_ph.kernels.edge_kernel import direct_edge_enumerate
 
@@ -242,9 +263,30 @@ def run_case(rips, case):
     return res, meta
 
 
+def make_thresholds():
+    """Reference auto_threshold / enclosing_radius values of THRESH_CASES."""
+    from flash_ph.threshold import auto_threshold, enclosing_radius
+
+    out = {}
+    for case in THRESH_CASES:
+        pts = make_points(case)
+        out[case["name"]] = {
+            "k": case["k"], "percentile": case["percentile"],
+            "auto_threshold": float(auto_threshold(pts, k=case["k"], percentile=case["percentile"])),
+            "enclosing_radius": float(enclosing_radius(pts)),
+        }
+        print(case["name"], json.dumps(out[case["name"]]), flush=True)
+    with open(os.path.join(HERE, "thresholds.json"), "w") as fh:
+        json.dump(out, fh, indent=1, sort_keys=True)
+
+
 def main():
-    rips = _load_reference()
-    only = set(sys.argv[1:])
+    argv = sys.argv[1:]
+    rips = _load_reference(_reference_src(argv))
+    if "--thresholds" in argv:
+        make_thresholds()
+        return
+    only = set(argv)
     manifest_path = os.path.join(HERE, "manifest.json")
     manifest = {}
     if os.path.exists(manifest_path):

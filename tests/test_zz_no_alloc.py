@@ -55,9 +55,12 @@ def test_noalloc_sort_matches_allocating_sort_on_consecutive_calls():
     stream = torch.cuda.current_stream().cuda_stream
     cap = lib.ph_edges_sort_noalloc_max_edges()
     assert cap == 1 << 19
-    # two calls in a row that share the static scratch; the second is larger
-    # and also exercises the colex-collision path (n > 92682)
-    for E, n, seed in ((70000, 5000, 1), (cap, 200000, 2)):
+    # Two calls in a row that both keep their scratch in the static array (the
+    # multi-launch radix form: more than 98,304 edges, n > 92682, which also
+    # takes the colex-collision path): the second, smaller call starts on the
+    # first call's leftover control block and look-back flags. A third call
+    # below the cluster form's limit (no scratch at all) closes the sequence.
+    for E, n, seed in ((cap, 200000, 2), (150000, 120000, 3), (70000, 5000, 1)):
         ei, ej, ed = _edges(E, n, seed)
         want = _allocating_sort(lib, ei, ej, ed, n, stream)
         got = _noalloc_sort(lib, ei, ej, ed, n, stream)
