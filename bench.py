@@ -273,30 +273,37 @@ def _thresholds(clouds):
 
 
 def _plain_stream(reqs, arrivals):
+    """Plain per-call rips_persistence, one request after another (each waits
+    for its arrival time). Returns completion times, per-request ok flags and
+    per-request service times (the call alone, arrival to completion when the
+    GPU was idle)."""
     import torch
     from flashph_b200 import rips_persistence
     t0 = time.perf_counter()
-    done, ok = [], 0
+    done, ok, service = [], [], []
     for (p, t, md), a in zip(reqs, arrivals):
         wait = t0 + a - time.perf_counter()
         if wait > 0:
             time.sleep(wait)
+        s0 = time.perf_counter()
         try:
             rips_persistence(p, t, max_dim=md)
-            ok += 1
+            ok.append(True)
         except ValueError:
-            pass
+            ok.append(False)
         torch.cuda.synchronize()
         done.append(time.perf_counter() - t0)
-    return np.asarray(done), ok
+        service.append(time.perf_counter() - s0)
+    return np.asarray(done), np.asarray(ok), np.asarray(service)
 
 
-def _served_stream(reqs, arrivals, slots=1):
+def _served_stream(reqs, arrivals, slots=None):
     from flashph_b200.serve import PersistenceServer
     t0 = time.perf_counter()
     done = [0.0] * len(reqs)
     futs = []
-    with PersistenceServer(slots=slots) as srv:
+    kw = {} if slots is None else {"slots": slots}
+    with PersistenceServer(**kw) as srv:
         for k, ((p, t, md), a) in enumerate(zip(reqs, arrivals)):
             wait = t0 + a - time.perf_counter()
             if wait > 0:
@@ -304,58 +311,73 @@ def _served_stream(reqs, arrivals, slots=1):
             f = srv.submit(p, t, md)
             f.add_done_callback(lambda _f, k=k: done.__setitem__(k, time.perf_counter() - t0))
             futs.append(f)
-        ok = 0
+        ok = []
         for f in futs:
             try:
                 f.result(timeout=600)
-                ok += 1
+                ok.append(True)
             except ValueError:
-                pass
-        batches = srv.batches
-    return np.asarray(done), ok, batches
+                ok.append(False)
+        sizes = list(srv.batch_sizes)
+    return np.asarray(done), np.asarray(ok), sizes
 
 
 def serving_summary(count, rates_rel=(0.5,), seed=7):
-    """Throughput (all requests queued at once) and latency at Poisson rates
-    given relative to the plain path's measured capacity."""
+    """Served against plain per-call rips_persistence on a seeded sample of the
+    serving stream: throughput in completed diagrams per second (requests over
+    the reference's limits are answered with its ValueError and are not
+    diagrams) with every request queued at once, each request's latency alone
+    on an idle GPU through the plain path, and p50/p99 latency under Poisson
+    arrivals at rates given relative to the plain path's request capacity."""
     reqs = serving_requests(count, seed)
     thr = _thresholds([r[0] for r in reqs])
     for r, t in zip(reqs, thr):
         r[1] = t
     # warm both paths over the whole request set: the first pass of a request
     # mix grows the device memory pool to its peak (for the served path, the
-    # peak of the requests in flight together), a one-time cost of any server
+    # peak of the batches in flight together), a one-time cost of any server
     _plain_stream(reqs, np.zeros(len(reqs)))
     _served_stream(reqs, np.zeros(len(reqs)))
     burst = np.zeros(count)
     # three alternating bursts per path, medians reported (a single burst varies
     # by tens of percent between runs)
-    plain_rates, served_rates = [], []
+    plain_rates, served_rates, plain_req_s, services = [], [], [], []
     for _ in range(3):
-        pd, pok = _plain_stream(reqs, burst)
-        sd, sok, nb = _served_stream(reqs, burst)
-        plain_rates.append(count / pd.max())
-        served_rates.append(count / sd.max())
+        pd, pok, service = _plain_stream(reqs, burst)
+        sd, sok, sizes = _served_stream(reqs, burst)
+        assert np.array_equal(pok, sok), "served and plain disagree on which requests are over a limit"
+        plain_rates.append(int(pok.sum()) / pd.max())
+        served_rates.append(int(sok.sum()) / sd.max())
+        plain_req_s.append(count / pd.max())
+        services.append(service)
     plain_rate = float(np.median(plain_rates))
     served_rate = float(np.median(served_rates))
-    out = {"requests": count, "ok": int(sok), "plain_ok": int(pok), "capped_or_invalid": int(count - sok),
+    single = np.median(np.stack(services), axis=0) * 1e3  # per request, ms
+    out = {"requests": count, "diagrams": int(sok.sum()), "over_limit": int(count - sok.sum()),
            "plain_diagrams_per_s": round(plain_rate, 2), "served_diagrams_per_s": round(served_rate, 2),
-           "served_over_plain": round(served_rate / plain_rate, 3), "served_batches_burst": int(nb),
+           "served_over_plain": round(served_rate / plain_rate, 3),
            "bursts": {"plain": [round(x, 1) for x in plain_rates], "served": [round(x, 1) for x in served_rates]},
+           "served_batches_burst": len(sizes), "served_batch_sizes": sorted(sizes, reverse=True)[:12],
+           "single_request_ms": {"p50": round(float(np.percentile(single, 50)), 3),
+                                 "p99": round(float(np.percentile(single, 99)), 3),
+                                 "max": round(float(single.max()), 3)},
            "rates": []}
     rng = np.random.default_rng(seed + 1)
+    req_rate = float(np.median(plain_req_s))
     for rel in rates_rel:
-        lam = rel * plain_rate
+        lam = rel * req_rate
         arr = np.cumsum(rng.exponential(1.0 / lam, count))
-        pd, _ = _plain_stream(reqs, arr)
-        sd, _, nb = _served_stream(reqs, arr)
+        pd, _, _ = _plain_stream(reqs, arr)
+        sd, _, sizes = _served_stream(reqs, arr)
         pl, sl = (pd - arr) * 1e3, (sd - arr) * 1e3
-        out["rates"].append({"rate_per_s": round(lam, 2), "rate_rel_plain_capacity": rel,
+        out["rates"].append({"requests_per_s": round(lam, 2), "rate_rel_plain_capacity": rel,
                              "plain_p50_ms": round(float(np.percentile(pl, 50)), 3),
                              "plain_p99_ms": round(float(np.percentile(pl, 99)), 3),
                              "served_p50_ms": round(float(np.percentile(sl, 50)), 3),
                              "served_p99_ms": round(float(np.percentile(sl, 99)), 3),
-                             "served_batches": int(nb)})
+                             "served_p99_over_single_p99": round(float(np.percentile(sl, 99)) /
+                                                                 out["single_request_ms"]["p99"], 3),
+                             "served_batches": len(sizes)})
     return out
 
 
@@ -446,140 +468,13 @@ def _fp64_errors(pts64, filt, dgms):
     return out
 
 
-def run_precision(args, rank, local):
-    """Precision form: rips_persistence on n x d N(0,1) points (default
-    200000 x 50, max_edge_length 6.0, max_dim 1). Edge enumeration with the
-    tensor-core screen against the direct FP32 kernel on the same GPU (edge
-    sets must be identical), the full call device-timed and end to end, and
-    the FP64 error of the diagrams' critical edge lengths."""
+def screened_kernel_ms(pts, t, flush, reps=3):
+    """Device time of the screened edge launch alone (ph_batch_edges_enumerate_screened,
+    as ph_rips_persistence makes it: one cloud, buffers prepared once, no host
+    read-back inside the events), median over reps after warm-up."""
     import torch
-    from flashph_b200 import _edges, _lib, _timing, rips_persistence
-    from flashph_b200.rips import enumerate_edges, rips_filtration
-
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    n, d, t, md = args.n or 200000, args.d or 50, args.t or 6.0, 1 if args.max_dim is None else args.max_dim
-    pts_np = np.random.default_rng(SEED + rank).standard_normal((n, d)).astype(np.float32)
-    pts = torch.from_numpy(pts_np).to(dev)
-    pinned = torch.from_numpy(pts_np).pin_memory()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-
-    def timed(fn, reps):
-        fn()
-        torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            r = fn()
-            b.record()
-            b.synchronize()
-            ts.append(a.elapsed_time(b))
-        return statistics.mean(ts), r
-
-    def canon(e):
-        i, j, dsq = e
-        key = i.long() * n + j.long()
-        o = torch.argsort(key)
-        return key[o], dsq[o].view(torch.int32)
-
-    scr_ms, es = timed(lambda: enumerate_edges(pts, t, screen=True, stats=True), max(3, args.steps))
-    stats = dict(_edges.last_screen_stats)
-    dir_ms, ed = timed(lambda: enumerate_edges(pts, t, screen=False), 3)
-    ka, da = canon(es)
-    kb, db = canon(ed)
-    identical = bool(ka.shape == kb.shape and torch.equal(ka, kb) and torch.equal(da, db))
-
-    steps = max(3, args.steps)
-    for _ in range(max(args.warmup, 3)):
-        rips_persistence(pts, t, max_dim=md)
-    torch.cuda.synchronize()
-    l0 = _lib.launch_count()
-    with ClockSampler(gpu_selector(local)) as clocks, _timing.record() as stages:
-        ms, out = timed(lambda: rips_persistence(pts, t, max_dim=md), steps)
-    launches = (_lib.launch_count() - l0) // (steps + 1)
-    e2e_ms, res = timed(lambda: rips_persistence(pinned, t, max_dim=md), max(3, steps // 2))
-    st = _timing.summarize(stages)
-
-    pairs = n * (n - 1) // 2
-    nt = (n + 127) // 128
-    tiles = nt * (nt + 1) // 2
-    kq = ((d + 4 + 15) // 16) * 16
-    tc_flops = 2.0 * 128 * 128 * kq * tiles
-    pk, src = peaks()
-    bf16_peak = pk.get("bf16_tflops", 1590.0)
-    filt = rips_filtration(pts, t)
-    errs = _fp64_errors(pts.double(), filt, out)
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        import oracle
-
-        oracle.build()
-        m = min(n, 40000)
-        cores = os.cpu_count() or 1
-        t0 = time.perf_counter()
-        oracle.run(pts_np[:m], t, md, fused=True, nthreads=cores)
-        sec = time.perf_counter() - t0
-        scale = (n * (n - 1)) / (m * (m - 1))
-        cpu = {"value": round(sec * 1e3 * scale, 1), "unit": "ms", "cores": cores, "kind": "port",
-               "sample": f"C++ port of the reference algorithm on the first {m} points "
-                         f"({sec:.2f} s), scaled by the pair count to n={n}"}
-    if rank == 0:
-        print(json.dumps({
-            "metric": f"{n // 1000}Kx{d} H0-H{md} ms (precision form)", "value": round(ms, 3), "unit": "ms",
-            "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 3), "higher_is_better": False,
-            "dtype": "f32 (bf16 screen)", "data": "synthetic",
-            "config": {"workload": f"rips_persistence, n={n} d={d} N(0,1) seed {SEED}, max_edge_length={t}, "
-                                   f"max_dim={md}", "l2": "flushed before every timed call (256 MiB write)"},
-            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(pinned.numel() * 4),
-                    "d2h_bytes_per_step": int(sum(r.numel() * 4 for r in res))},
-            "gpu_launches": int(launches),
-            "edges": {"E": int(ka.shape[0]), "pairs": pairs, "screened_ms": round(scr_ms, 3),
-                      "direct_ms": round(dir_ms, 3), "speedup": round(dir_ms / scr_ms, 2),
-                      "identical_to_direct": identical, "screen_candidates": stats["candidates"],
-                      "forced_pairs": stats["forced"],
-                      "candidates_per_edge": round(stats["candidates"] / max(1, int(ka.shape[0])), 3)},
-            "roofline": {"kernel": "k_tc_edges (tensor-core screened edge enumeration, with its prep kernels)",
-                         "bound": "tensor", "achieved": round(tc_flops / (scr_ms * 1e-3) / 1e12, 2),
-                         "peak": bf16_peak, "unit": "TFLOP/s",
-                         "frac": round(tc_flops / (scr_ms * 1e-3) / 1e12 / bf16_peak, 4), "traffic": None,
-                         "algorithmic_flops_per_launch": tc_flops, "avg_launch_ms": round(scr_ms, 4)},
-            "tensor": {"mma_flops": tc_flops, "tflops": round(tc_flops / (scr_ms * 1e-3) / 1e12, 2),
-                       "peak_bf16_tflops": bf16_peak, "frac": round(tc_flops / (scr_ms * 1e-3) / 1e12 / bf16_peak, 4),
-                       "peak_source": src},
-            "stages_ms": {k: round(v[1] / max(v[0], 1), 4) for k, v in st.items()},
-            "fp64_error": errs,
-            "rows": [int(o.shape[0]) for o in out],
-            "cpu_baseline": cpu, "clocks": clocks.summary()}), flush=True)
-
-
-def kernel_breakdown(pts, t, max_dim, flush, reps=3):
-    """Per-stage device times of the staged pipeline (CUDA events around each
-    stage's launches) and of the screened edge kernel alone, plus the sizes
-    the algorithmic byte and flop counts need. Runs outside the timed region."""
-    import torch
-    from flashph_b200 import _timing, rips_persistence
-    from flashph_b200.cohomology import enumerate_triangles
-    from flashph_b200.rips import enumerate_edges, rips_filtration
-
-    os.environ["FLASHPH_PIPELINE"] = "staged"
-    try:
-        rips_persistence(pts, t, max_dim=max_dim)
-        with _timing.record() as ev:
-            for _ in range(reps):
-                flush.zero_()
-                rips_persistence(pts, t, max_dim=max_dim)
-            torch.cuda.synchronize()
-        st = _timing.summarize(ev)
-    finally:
-        os.environ.pop("FLASHPH_PIPELINE", None)
-    stages = {k: v[1] / max(v[0], 1) for k, v in st.items()}
-    # the screened edge launches alone (as ph_rips_persistence makes them),
-    # buffers prepared once, no host read-back inside the events
-    import numpy as np
     from flashph_b200 import _lib as L
-    from flashph_b200.rips import _SEG_DTYPE, threshold_sq
+    from flashph_b200.rips import _SEG_DTYPE, enumerate_edges, threshold_sq
     n, d = pts.shape
     seg = np.zeros(1, dtype=_SEG_DTYPE)
     seg[0] = (0, 0, 0, n, d, threshold_sq(t), 1)
@@ -605,7 +500,177 @@ def kernel_breakdown(pts, t, max_dim, flush, reps=3):
         b.record()
         b.synchronize()
         ts.append(a.elapsed_time(b))
-    edge_ms = statistics.median(ts[2:])
+    assert int(stt.item()) == 0
+    return statistics.median(ts[3:])
+
+
+def tc_mma_flops(n, d):
+    """MMA flops the screened kernel issues: 2 x 128 x 128 x 16*ceil((d+4)/16)
+    per 128 x 128 point tile, nt(nt+1)/2 tiles."""
+    nt = (n + 127) // 128
+    return 2.0 * 128 * 128 * (((d + 4 + 15) // 16) * 16) * nt * (nt + 1) / 2
+
+
+def precision_summary(dev, n, d, t, md, steps, warmup, seed=SEED, clock_sel=None):
+    """Precision form on n x d N(0,1) points: the screened edge kernel against
+    the direct FP32 kernel (identical edge sets required), the tensor-core
+    roofline of the screened launch alone, the full call device-timed (L2
+    flushed) and end to end, and the FP64 error of the diagrams' critical edge
+    lengths."""
+    import torch
+    from flashph_b200 import _edges, _lib, _timing, rips_persistence
+    from flashph_b200.rips import enumerate_edges, rips_filtration
+
+    pts_np = np.random.default_rng(seed).standard_normal((n, d)).astype(np.float32)
+    pts = torch.from_numpy(pts_np).to(dev)
+    pinned = torch.from_numpy(pts_np).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            r = fn()
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.mean(ts), r
+
+    def canon(e):
+        i, j, dsq = e
+        key = i.long() * n + j.long()
+        o = torch.argsort(key)
+        return key[o], dsq[o].view(torch.int32)
+
+    es = enumerate_edges(pts, t, screen=True, stats=True)
+    stats = dict(_edges.last_screen_stats)
+    dir_ms, ed = timed(lambda: enumerate_edges(pts, t, screen=False), 3)
+    ka, da = canon(es)
+    kb, db = canon(ed)
+    identical = bool(ka.shape == kb.shape and torch.equal(ka, kb) and torch.equal(da, db))
+    kern_ms = screened_kernel_ms(pts, t, flush, reps=max(3, min(steps, 10)))
+
+    for _ in range(max(warmup, 3)):
+        rips_persistence(pts, t, max_dim=md)
+    torch.cuda.synchronize()
+    l0 = _lib.launch_count()
+    clocks = None
+    with _timing.record() as stages:
+        if clock_sel is not None:
+            with ClockSampler(clock_sel) as cs:
+                ms, out = timed(lambda: rips_persistence(pts, t, max_dim=md), steps)
+            clocks = cs.summary()
+        else:
+            ms, out = timed(lambda: rips_persistence(pts, t, max_dim=md), steps)
+    launches = (_lib.launch_count() - l0) // (steps + 1)
+    e2e_ms, res = timed(lambda: rips_persistence(pinned, t, max_dim=md), max(3, steps // 2))
+    st = _timing.summarize(stages)
+
+    tc_flops = tc_mma_flops(n, d)
+    pk, src = peaks()
+    bf16_peak = pk.get("bf16_tflops", 1590.0)
+    tf = tc_flops / (kern_ms * 1e-3) / 1e12
+    filt = rips_filtration(pts, t)
+    errs = _fp64_errors(pts.double(), filt, out)
+    return {
+        "pts_np": pts_np, "ms": ms, "e2e_ms": e2e_ms, "launches": launches, "clocks": clocks,
+        "h2d": int(pinned.numel() * 4), "d2h": int(sum(r.numel() * 4 for r in res)),
+        "rows": [int(o.shape[0]) for o in out],
+        "stages_ms": {k: round(v[1] / max(v[0], 1), 4) for k, v in st.items()},
+        "edges": {"E": int(ka.shape[0]), "pairs": n * (n - 1) // 2, "screened_kernel_ms": round(kern_ms, 4),
+                  "direct_ms": round(dir_ms, 3), "speedup": round(dir_ms / kern_ms, 2),
+                  "identical_to_direct": identical, "screen_candidates": stats["candidates"],
+                  "forced_pairs": stats["forced"],
+                  "candidates_per_edge": round(stats["candidates"] / max(1, int(ka.shape[0])), 3)},
+        "tensor": {"kernel": "k_tc_edges (tensor-core screened edge enumeration, with its prep launches)",
+                   "bound": "tensor", "achieved": round(tf, 2), "peak": bf16_peak, "unit": "TFLOP/s",
+                   "frac": round(tf / bf16_peak, 4), "algorithmic_flops_per_launch": tc_flops,
+                   "avg_launch_ms": round(kern_ms, 4),
+                   "per_unit": "2 x 128 x 128 x 16*ceil((d+4)/16) MMA flops per 128x128 point tile, "
+                               "nt(nt+1)/2 tiles",
+                   "peak_source": f"bf16_tflops burst ({src} peaks file)"},
+        "fp64_error": errs,
+    }
+
+
+def precision_block(dev, steps=5, warmup=3):
+    """The precision configuration (200000 x 50, t=6.0, H0-H1) as a sub-block
+    of the default line."""
+    p = precision_summary(dev, 200000, 50, 6.0, 1, steps, warmup)
+    return {"workload": "rips_persistence, n=200000 d=50 N(0,1) seed 42, max_edge_length=6.0, max_dim=1",
+            "call_ms": round(p["ms"], 3), "e2e_ms": round(p["e2e_ms"], 3),
+            "identical_to_direct": p["edges"]["identical_to_direct"], "edges": p["edges"],
+            "tensor": p["tensor"], "fp64_error": p["fp64_error"], "rows": p["rows"]}
+
+
+def run_precision(args, rank, local):
+    """Precision form as its own line: rips_persistence on n x d N(0,1)
+    points (default 200000 x 50, max_edge_length 6.0, max_dim 1)."""
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, d, t, md = args.n or 200000, args.d or 50, args.t or 6.0, 1 if args.max_dim is None else args.max_dim
+    steps = max(3, args.steps)
+    p = precision_summary(dev, n, d, t, md, steps, args.warmup, seed=SEED + rank, clock_sel=gpu_selector(local))
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        oracle.build()
+        m = min(n, 40000)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.run(p["pts_np"][:m], t, md, fused=True, nthreads=cores)
+        sec = time.perf_counter() - t0
+        scale = (n * (n - 1)) / (m * (m - 1))
+        cpu = {"value": round(sec * 1e3 * scale, 1), "unit": "ms", "cores": cores, "kind": "port",
+               "sample": f"C++ port of the reference algorithm on the first {m} points "
+                         f"({sec:.2f} s), scaled by the pair count to n={n}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"{n // 1000}Kx{d} H0-H{md} ms (precision form)", "value": round(p["ms"], 3), "unit": "ms",
+            "n_gpus": 1, "steps": steps, "warmup": max(args.warmup, 3), "higher_is_better": False,
+            "dtype": "f32 (bf16 screen)", "data": "synthetic",
+            "config": {"workload": f"rips_persistence, n={n} d={d} N(0,1) seed {SEED}, max_edge_length={t}, "
+                                   f"max_dim={md}", "l2": "flushed before every timed call (256 MiB write)"},
+            "e2e": {"value": round(p["e2e_ms"], 3), "unit": "ms", "h2d_bytes_per_step": p["h2d"],
+                    "d2h_bytes_per_step": p["d2h"]},
+            "gpu_launches": int(p["launches"]),
+            "edges": p["edges"],
+            "roofline": dict(p["tensor"], traffic=None),
+            "stages_ms": p["stages_ms"],
+            "fp64_error": p["fp64_error"],
+            "rows": p["rows"],
+            "cpu_baseline": cpu, "clocks": p["clocks"]}), flush=True)
+
+
+def kernel_breakdown(pts, t, max_dim, flush, reps=3):
+    """Per-stage device times of the staged pipeline (CUDA events around each
+    stage's launches) and of the screened edge kernel alone, plus the sizes
+    the algorithmic byte and flop counts need. Runs outside the timed region."""
+    import torch
+    from flashph_b200 import _timing, rips_persistence
+    from flashph_b200.cohomology import enumerate_triangles
+    from flashph_b200.rips import enumerate_edges, rips_filtration
+
+    os.environ["FLASHPH_PIPELINE"] = "staged"
+    try:
+        rips_persistence(pts, t, max_dim=max_dim)
+        with _timing.record() as ev:
+            for _ in range(reps):
+                flush.zero_()
+                rips_persistence(pts, t, max_dim=max_dim)
+            torch.cuda.synchronize()
+        st = _timing.summarize(ev)
+    finally:
+        os.environ.pop("FLASHPH_PIPELINE", None)
+    stages = {k: v[1] / max(v[0], 1) for k, v in st.items()}
+    edge_ms = screened_kernel_ms(pts, t, flush, reps=reps)
     filt = rips_filtration(pts, t)
     E = int(filt.edge_i.shape[0])
     T = enumerate_triangles(filt).T if max_dim >= 1 else 0
@@ -622,9 +687,7 @@ NCU_TRAFFIC = {
 
 def rooflines(stages, edge_ms, n, d, E, T, pk, src):
     """Roofline entries of the three kernels that dominate the call."""
-    nt = (n + 127) // 128
-    ks = (d + 4 + 15) // 16
-    mma_flops = 2.0 * 128 * 128 * 16 * ks * nt * (nt + 1) / 2
+    mma_flops = tc_mma_flops(n, d)
     tf = mma_flops / (edge_ms * 1e-3) / 1e12
     bf16 = pk.get("bf16_tflops", 1590.0)
     hbm = pk.get("hbm_gbs", 6650.0)
@@ -728,6 +791,7 @@ def main():
     ap.add_argument("--impl", choices=("flashph", "reference"), default="flashph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=96)
     ap.add_argument("--workload", choices=("plain", "batch", "serve", "precision"), default="plain")
     ap.add_argument("--clouds", type=int, default=4096)
@@ -857,8 +921,10 @@ def main():
                              "native pipeline",
             "sizes": {"edges": E, "triangles": T},
         }
-        if not args.no_serving and world == 1:  # a one-GPU sub-measurement
+        if not args.no_serving and world == 1:  # one-GPU sub-measurements
             line["serving"] = serving_summary(args.serving_requests, rates_rel=(0.5,))
+        if not args.no_precision and world == 1:
+            line["precision"] = precision_block(dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -7,11 +7,14 @@
 // buffers come from the stream-ordered allocator and are released together.
 // The host waits only where a count decides the next allocation:
 //   1. the edge count (edge buffers are sized by an estimate, rerun if short)
+//   1b. on dense graphs, the exact triangle total (checked against the limit
+//       before the filtration order and the forest are built)
 //   2. the triangle count (and the H0 forest's status)
 //   3. the H1 reduction's status and row count, together with the
 //      tetrahedron count when H2 is asked for
 //   4. the H2 reduction's status and row count
 // The results stay on the device in a ph_result until copied out.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -20,7 +23,7 @@
 #include <string>
 #include <vector>
 
-#include "prim.cuh"
+#include "pipeline.cuh"
 
 using namespace ph;
 
@@ -35,52 +38,59 @@ struct ph_result {
   std::vector<void*> scratch;
 };
 
-namespace {
+namespace ph {
+namespace pl {
 
-// stream-ordered allocations released together when the run ends
-struct Arena {
-  cudaStream_t s;
-  std::vector<void*> ptrs;
-  bool failed = false;
-  explicit Arena(cudaStream_t st) : s(st) {}
-  Arena(const Arena&) = delete;
-  Arena& operator=(const Arena&) = delete;
-  template <typename T>
-  T* take(i64 count) {
-    void* p = nullptr;
-    const size_t bytes = (size_t)std::max<i64>(count, 1) * sizeof(T);
-    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) {
-      failed = true;
-      return nullptr;
-    }
-    ptrs.push_back(p);
-    return static_cast<T*>(p);
-  }
-  void* bytes(size_t n) { return take<unsigned char>((i64)std::max<size_t>(n, 1)); }
-  // hands the buffers to a result, which frees them later
-  void release_to(ph_result* r) {
-    r->scratch.swap(ptrs);
-    ptrs.clear();
-  }
-  ~Arena() {
-    for (void* p : ptrs) cudaFreeAsync(p, s);
-  }
-};
-
-// Small pinned, device-mapped host buffers for count and status readbacks (a
-// kernel writes the values into them directly). They come from a process-wide
-// pool: a call takes one and returns it, so host threads that come and go (a
-// server's worker slots) do not allocate pinned memory, which can wait for the
-// whole device, on their first call.
-struct Slots {
-  int64_t* host = nullptr;
-  int64_t* dev = nullptr;
-  int64_t* seq = nullptr;  // host-side count of readbacks through this buffer
-};
+namespace detail {
 constexpr int kSeqSlot = 8;  // word the readback kernel writes last
 std::mutex g_slots_mu;
 std::vector<Slots> g_slots_free;
+std::mutex g_pinned_mu;
+std::vector<Pinned> g_pinned_free;
 
+// copies up to four device int64 values into the mapped host slots
+__global__ void k_report(const int64_t* a, const int64_t* b, const int64_t* c, const int64_t* d, int count,
+                         volatile int64_t* out, int64_t seq) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  const int64_t* src[4] = {a, b, c, d};
+  if (threadIdx.x < count && threadIdx.x < 4) out[threadIdx.x] = *src[threadIdx.x];
+  __threadfence_system();
+  __syncwarp();
+  // the sequence word last: the host reads the values once it sees it
+  if (threadIdx.x == 0) out[kSeqSlot] = seq;
+  __threadfence_system();
+}
+
+// spins on the sequence word in host memory for up to half a millisecond (no
+// driver call, so concurrent callers on other threads do not contend for the
+// driver while waiting; the usual wait is a few microseconds, and a blocking
+// wait adds its wake-up latency to every readback), then blocks
+int wait_seq(const Slots& dst, int64_t seq, cudaStream_t s) {
+  volatile int64_t* flag = dst.host + kSeqSlot;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int it = 0;; ++it) {
+    if (*flag == seq) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      return PH_OK;
+    }
+    if ((it & 255) == 255 && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(500)) break;
+  }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    record_error(e);
+    return PH_ERR_CUDA;
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return PH_OK;
+}
+}  // namespace detail
+using namespace detail;
+
+// Readback buffers come from a process-wide pool: a call takes one and
+// returns it, so host threads that come and go (a server's worker slots) do
+// not allocate pinned memory, which can wait for the whole device, on their
+// first call.
 Slots take_slots() {
   {
     std::lock_guard<std::mutex> lock(g_slots_mu);
@@ -104,27 +114,36 @@ Slots take_slots() {
   return b;
 }
 
-struct SlotsLease {
-  Slots b = take_slots();
-  ~SlotsLease() {
-    if (!b.host) return;
-    std::lock_guard<std::mutex> lock(g_slots_mu);
-    g_slots_free.push_back(b);
-  }
-};
+void give_slots(const Slots& b) {
+  std::lock_guard<std::mutex> lock(g_slots_mu);
+  g_slots_free.push_back(b);
+}
 
-// copies up to four device int64 values into the mapped host slots
-__global__ void k_report(const int64_t* a, const int64_t* b, const int64_t* c, const int64_t* d, int count,
-                         volatile int64_t* out, int64_t seq) {
-  ph::pdl_wait();
-  ph::pdl_trigger();
-  const int64_t* src[4] = {a, b, c, d};
-  if (threadIdx.x < count && threadIdx.x < 4) out[threadIdx.x] = *src[threadIdx.x];
-  __threadfence_system();
-  __syncwarp();
-  // the sequence word last: the host reads the values once it sees it
-  if (threadIdx.x == 0) out[kSeqSlot] = seq;
-  __threadfence_system();
+Pinned take_pinned(size_t bytes) {
+  bytes = std::max<size_t>(bytes, 4096);
+  {
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    // the smallest free buffer that is large enough
+    int best = -1;
+    for (int i = 0; i < (int)g_pinned_free.size(); ++i)
+      if (g_pinned_free[i].bytes >= bytes && (best < 0 || g_pinned_free[i].bytes < g_pinned_free[best].bytes)) best = i;
+    if (best >= 0) {
+      const Pinned p = g_pinned_free[best];
+      g_pinned_free.erase(g_pinned_free.begin() + best);
+      return p;
+    }
+  }
+  size_t sz = 4096;
+  while (sz < bytes) sz <<= 1;
+  Pinned p;
+  if (cudaHostAlloc(&p.host, sz, cudaHostAllocPortable) != cudaSuccess) return Pinned{};
+  p.bytes = sz;
+  return p;
+}
+
+void give_pinned(const Pinned& p) {
+  std::lock_guard<std::mutex> lock(g_pinned_mu);
+  g_pinned_free.push_back(p);
 }
 
 // keeps the device's stream-ordered pool from returning memory at every sync
@@ -143,7 +162,6 @@ void keep_pool(int dev) {
   });
 }
 
-// fp32 of a double, round to nearest even, inf beyond the fp32 range (numpy's float32())
 float to_f32(double v) {
   if (std::isnan(v)) return NAN;
   const double lim = 0x1p128 - 0x1p103;  // halfway between FLT_MAX and 2^128
@@ -151,6 +169,70 @@ float to_f32(double v) {
   if (v <= -lim) return -INFINITY;
   return (float)v;
 }
+
+int fail(int code, const std::string& msg) {
+  record_message(msg.c_str());
+  return code;
+}
+
+int readback(const int64_t* const* src, int count, const Slots& dst, cudaStream_t s) {
+  const int64_t seq = ++*dst.seq;
+  count_launch();
+  if (ph::launch_pdl(k_report, dim3(1), dim3(32), 0, s, src[0], count > 1 ? src[1] : src[0],
+                     count > 2 ? src[2] : src[0], count > 3 ? src[3] : src[0], count, dst.dev,
+                     seq) != cudaSuccess) {
+    record_error(cudaGetLastError());
+    return PH_ERR_CUDA;
+  }
+  return wait_seq(dst, seq, s);
+}
+
+int readback_parts(const Part* parts, int nparts, const Slots& slots, cudaStream_t s) {
+  for (int k = 0; k < nparts; ++k) {
+    if (!parts[k].bytes) continue;
+    const cudaError_t e = cudaMemcpyAsync(parts[k].dst, parts[k].src, parts[k].bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) {
+      record_error(e);
+      return PH_ERR_CUDA;
+    }
+  }
+  // the copies precede the report kernel in stream order: when its sequence
+  // word arrives, every part is in host memory
+  const int64_t seq = ++*slots.seq;
+  count_launch();
+  if (ph::launch_pdl(k_report, dim3(1), dim3(32), 0, s, (const int64_t*)nullptr, (const int64_t*)nullptr,
+                     (const int64_t*)nullptr, (const int64_t*)nullptr, 0, slots.dev, seq) != cudaSuccess) {
+    record_error(cudaGetLastError());
+    return PH_ERR_CUDA;
+  }
+  return wait_seq(slots, seq, s);
+}
+
+i64 pool_capacity(i64 nnz, i64 K) {
+  const i64 mult = nnz < (i64(1) << 24) ? 8 : 3;
+  return std::min<i64>(mult * nnz + 2 * K + (i64(1) << 23), POOL_MAX);
+}
+
+int reduce_only(Arena& A, cudaStream_t s, const i32* off, const i32* data, i64 K, i32 col_base, i64 R,
+                i32 row_base, i64 span, const uint8_t* skip, const i32* cmf, i64 pool_cap, int* status, RedOut& o) {
+  o.state = A.take<i32>(K);
+  o.piv = A.take<i32>(K);
+  o.info = A.take<int64_t>(4);
+  o.nrows = A.take<int64_t>(1);
+  i32* pool = A.take<i32>(pool_cap);
+  const size_t rb = ph_reduce_workspace_bytes(K, R, span);
+  void* rws = A.bytes(rb);
+  if (A.failed) return fail(PH_ERR_CUDA, "rips_persistence: device allocation failed");
+  return ph_reduce(off, data, K, col_base, R, row_base, span, skip, cmf, o.state, o.piv, pool, pool_cap, o.info,
+                   status, rws, rb, s);
+}
+
+}  // namespace pl
+}  // namespace ph
+
+using namespace ph::pl;
+
+namespace {
 
 // the segment record of a single cloud, and the run's counters cleared
 __global__ void k_single_seg(ph_cloud_seg* seg, int64_t* blk_off, int64_t n, int32_t d, float thr_sq,
@@ -171,76 +253,14 @@ __global__ void k_single_seg(ph_cloud_seg* seg, int64_t* blk_off, int64_t n, int
   blk_off[1] = nblocks;
 }
 
-int fail(int code, const std::string& msg) {
-  record_message(msg.c_str());
-  return code;
-}
-
-// brings count (<= 4) int64 values from the device into the pinned slots (one
-// kernel writes them into the mapped host buffer, then a sequence word) and
-// waits: spins on the sequence word for up to half a millisecond (the usual
-// wait is a few microseconds, and a blocking wait adds its wake-up latency to
-// every readback), then blocks
-int readback(const int64_t* const* src, int count, const Slots& dst, cudaStream_t s) {
-  const int64_t seq = ++*dst.seq;
-  count_launch();
-  if (ph::launch_pdl(k_report, dim3(1), dim3(32), 0, s, src[0], count > 1 ? src[1] : src[0],
-                     count > 2 ? src[2] : src[0], count > 3 ? src[3] : src[0], count, dst.dev,
-                     seq) != cudaSuccess) {
-    record_error(cudaGetLastError());
-    return PH_ERR_CUDA;
-  }
-  // spin on the sequence word in host memory (no driver call, so concurrent
-  // callers on other threads do not contend for the driver while waiting)
-  volatile int64_t* flag = dst.host + kSeqSlot;
-  const auto t0 = std::chrono::steady_clock::now();
-  for (int it = 0;; ++it) {
-    if (*flag == seq) {
-      std::atomic_thread_fence(std::memory_order_acquire);
-      return PH_OK;
-    }
-    if ((it & 255) == 255 && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(500)) break;
-  }
-  // a long stage: block, then the word is there (or the stream reports an error)
-  const cudaError_t e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) {
-    record_error(e);
-    return PH_ERR_CUDA;
-  }
-  std::atomic_thread_fence(std::memory_order_acquire);
-  return PH_OK;
-}
-
-// reduction pool (int32 entries): initial records (at most 2 nnz), per-warp
-// chunks, reduced columns; bounded by the 33-bit record offsets
-constexpr i64 POOL_MAX = (i64(1) << 33) - 1;
-i64 pool_capacity(i64 nnz, i64 K) {
-  const i64 mult = nnz < (i64(1) << 24) ? 8 : 3;
-  return std::min<i64>(mult * nnz + 2 * K + (i64(1) << 23), POOL_MAX);
-}
-
-struct RedOut {
-  i32* state;
-  i32* piv;
-  int64_t* info;
-  int64_t* nrows;
-};
-
 // one reduction (H1 or H2) and its persistence rows, enqueued
 int reduce_rows(Arena& A, cudaStream_t s, const i32* off, const i32* data, i64 K, i32 col_base, i64 R,
                 i32 row_base, const uint8_t* skip, const i32* cmf, const float* filt, const i32* col_m,
                 const i32* row_m, i64 pool_cap, int* status, float* rows, RedOut& o) {
-  o.state = A.take<i32>(K);
-  o.piv = A.take<i32>(K);
-  o.info = A.take<int64_t>(4);
-  o.nrows = A.take<int64_t>(1);
-  i32* pool = A.take<i32>(pool_cap);
-  const size_t rb = ph_reduce_workspace_bytes(K, R), pb = ph_persistence_rows_workspace_bytes(K);
-  void* rws = A.bytes(rb);
+  PH_TRY(reduce_only(A, s, off, data, K, col_base, R, row_base, R, skip, cmf, pool_cap, status, o));
+  const size_t pb = ph_persistence_rows_workspace_bytes(K);
   void* pws = A.bytes(pb);
   if (A.failed) return fail(PH_ERR_CUDA, "rips_persistence: device allocation failed");
-  PH_TRY(ph_reduce(off, data, K, col_base, R, row_base, skip, cmf, o.state, o.piv, pool, pool_cap, o.info, status,
-                   rws, rb, s));
   return ph_persistence_rows(o.state, o.piv, K, row_base, filt, col_m, row_m, rows, o.nrows, pws, pb, s);
 }
 
@@ -294,7 +314,11 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   const size_t ews = screened ? ph_edges_screened_workspace_bytes(n, 1, d) : 0;
   void* ew = screened ? A.bytes(ews) : nullptr;
   const i64 pairs = n * (n - 1) / 2;
-  i64 cap = std::min<i64>(pairs, std::max<i64>(1 << 22, 256 * n));
+  // first edge buffer: 256 edges a point, 2^22 at least, and up to an eighth
+  // of the pairs (at most 2^27 edges, 1.5 GiB): dense clouds (thresholds at
+  // a k-NN percentile in high d keep a few percent of all pairs) then fit the
+  // first pass instead of enumerating twice
+  i64 cap = std::min<i64>(pairs, std::max<i64>({i64(1) << 22, 256 * n, std::min<i64>(pairs / 8, i64(1) << 27)}));
   i32 *ei = nullptr, *ej = nullptr;
   float* ed = nullptr;
   i64 E = 0;
@@ -335,6 +359,39 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     return give_up(fail(PH_ERR_CAPACITY, m));
   }
   res->stats[0] = E;
+
+  // ---- 1b. dense graphs: the exact triangle total first --------------------------------------
+  // On dense graphs the per-edge triangle count costs sum(deg^2), and a call
+  // over the triangle limit (the reference's ValueError, with the exact total
+  // in its text) needs nothing but that total: it comes from a rank-free
+  // adjacency of the unsorted edges and a shared-bitmap pass, before the
+  // filtration order and the forest are built.
+  const bool total_first = max_dim >= 1 && 4.0 * (double)E * (double)E / (double)n > 2e8 &&
+                           n <= ph_triangles_total_max_vertices();
+  i64 T_total = -1;
+  if (total_first) {
+    i32* tp = A.take<i32>(n + 1);
+    i32* tidx = A.take<i32>(2 * E);
+    i32* trank = A.take<i32>(2 * E);
+    const size_t tcsr_b = ph_vertex_csr_workspace_bytes(E);
+    void* tcsr_ws = A.bytes(tcsr_b);
+    if (A.failed) return alloc_fail();
+    int rc = ph_vertex_csr(ei, ej, E, n, tp, tidx, trank, tcsr_ws, tcsr_b, s);
+    if (rc == PH_OK)
+      rc = ph_triangles_total(tp, tidx, n, reinterpret_cast<unsigned long long*>(cnt + 5),
+                              reinterpret_cast<int*>(cnt + 6), s);
+    if (rc != PH_OK) return give_up(rc);
+    const int64_t* src[1] = {cnt + 5};
+    if (readback(src, 1, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    T_total = H[0];
+    if (T_total > max_triangles) {
+      char m[200];
+      snprintf(m, sizeof m,
+               "Triangle count %lld exceeds max_triangles=%lld. Reduce max_edge_length or increase max_triangles.",
+               (long long)T_total, (long long)max_triangles);
+      return give_up(fail(PH_ERR_LIMIT, m));
+    }
+  }
 
   // ---- 2. filtration order, adjacency, values ---------------------------------------------
   i32* si = A.take<i32>(E);
@@ -377,7 +434,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (readback(src, 1, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_mst = (int)(H[0] >> 32);
     if (st_mst) return give_up(fail(st_mst, "ph_boruvka_mst failed"));
-    A.release_to(res);
+    A.release_to(res->scratch);
     *out = res;
     return PH_OK;
   }
@@ -388,18 +445,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   const size_t tc_b = ph_triangles_count_workspace_bytes(E);
   void* tc_ws = A.bytes(tc_b);
   if (A.failed) return alloc_fail();
-  // On dense graphs the per-edge count costs sum(deg^2); the exact total comes
-  // first from a cheaper rank-free pass, so that a call over the triangle
-  // limit fails without the per-edge pass.
-  const bool total_first =
-      4.0 * (double)E * (double)E / (double)n > 2e8 && n <= ph_triangles_total_max_vertices();
-  if (total_first) {
-    int rc = ph_triangles_total(adj_ptr, adj_idx, n, reinterpret_cast<unsigned long long*>(cnt + 5),
-                                reinterpret_cast<int*>(cnt + 6), s);
-    if (rc != PH_OK) return give_up(rc);
-    const int64_t* src[2] = {cnt + 5, cnt + 1};
-    if (readback(src, 2, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
-  } else {
+  {
     int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[2] = {tri_off + E, cnt + 1};
@@ -407,6 +453,12 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   }
   const i64 T = H[0];
   if ((int)(H[1] >> 32) != 0) return give_up(fail((int)(H[1] >> 32), "ph_boruvka_mst failed"));
+  if (T_total >= 0 && T != T_total) {
+    char m[160];
+    snprintf(m, sizeof m, "triangle counts disagree: %lld per edge, %lld in total", (long long)T,
+             (long long)T_total);
+    return give_up(fail(PH_ERR_ARG, m));
+  }
   if (T > max_triangles) {
     char m[200];
     snprintf(m, sizeof m,
@@ -420,10 +472,6 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     return give_up(fail(PH_ERR_LIMIT, m));
   }
   res->stats[1] = T;
-  if (total_first) {  // per-edge counts for the emission offsets (their sum is T)
-    int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
-    if (rc != PH_OK) return give_up(rc);
-  }
   i32* tri_m = A.take<i32>(T);
   i32* tri_w = A.take<i32>(T);
   i32* tri_fa = A.take<i32>(T);
@@ -478,7 +526,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   res->nrows[1] = H[1];
   res->stats[3] = H[2];
   if (max_dim == 1) {
-    A.release_to(res);
+    A.release_to(res->scratch);
     *out = res;
     return PH_OK;
   }
@@ -538,7 +586,7 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   }
   res->nrows[2] = H[2];
   res->stats[4] = H[3];
-  A.release_to(res);
+  A.release_to(res->scratch);
   *out = res;
   return PH_OK;
 }

@@ -433,8 +433,22 @@ __device__ __forceinline__ unsigned long long pool_alloc(PoolChunk& ch, RedCtl* 
 // fits one of the warp's shared buffers (up to 32 * RD_CAP rows) every
 // working column is such a bitmap in shared memory; otherwise only a column
 // that outgrows its shared buffer becomes one, in a global slot per warp.
+//
+// A global bitmap spans the whole row range (millions of rows for dense
+// complexes), while a column's entries are a few thousand at most: scanning
+// it word by word for the next pivot, the record or the clear would cost the
+// range, not the column. Global bitmaps therefore carry a summary in the
+// warp's shared memory: bit b of summary word s is set when data words
+// [32 (32 s + b), 32 (32 s + b) + 32) (1024 rows, one warp-wide load) may hold
+// set bits. Flips set summary bits; scans visit only the blocks whose bits
+// are set and drop the bits of blocks found empty; clearing a column zeroes
+// only its blocks.
+constexpr int RD_SUM_WORDS = RD_CAPB;  // summary words (the added-column buffer, idle while the column is a bitmap)
+
 struct DenseCol {
   u32* bits = nullptr;  // this warp's bitmap
+  u32* sum = nullptr;   // summary of a global bitmap (shared memory), null for a shared bitmap
+  i32 rb = 0;           // rank of the bitmap's bit 0 (word-aligned, at or below the column's first pivot)
   i64 lo = 0, hi = -1;  // touched word range
   i32 piv = -1;         // lowest set bit (global rank)
   bool sm = false;      // bits are in this warp's shared memory
@@ -456,6 +470,16 @@ __device__ __forceinline__ u32 sm_xor32(u32* p, u32 x) {
 __device__ __forceinline__ void sm_red_xor32(u32* p, u32 x) {
   asm volatile("red.shared.xor.b32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(x) : "memory");
 }
+__device__ __forceinline__ void sm_red_or32(u32* p, u32 x) {
+  asm volatile("red.shared.or.b32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(x) : "memory");
+}
+__device__ __forceinline__ void sm_red_and32(u32* p, u32 x) {
+  asm volatile("red.shared.and.b32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(x) : "memory");
+}
+__device__ __forceinline__ void gl_red_xor32(u32* p, u32 x) {
+  asm volatile("red.relaxed.gpu.global.xor.b32 [%0], %1;" ::"l"(p), "r"(x) : "memory");
+}
+
 __device__ __forceinline__ void sm_st32(u32* p, u32 v) {
   asm volatile("st.shared.u32 [%0], %1;" ::"r"((u32)__cvta_generic_to_shared(p)), "r"(v) : "memory");
 }
@@ -476,9 +500,14 @@ __device__ void dense_flip_regs(DenseCol& D, i32 v, int len, i32 row_base) {
   if (lane < len) {
     const i32 e = v - row_base;
     const u32 b = 1u << (e & 31);
-    if (D.sm) sm_red_xor32(D.bits + (e >> 5), b);
-    else atomicXor(D.bits + (e >> 5), b);
+    if (D.sm) {
+      sm_red_xor32(D.bits + (e >> 5), b);
+    } else {
+      gl_red_xor32(D.bits + (e >> 5), b);
+      if (D.sum) sm_red_or32(D.sum + (e >> 15), 1u << ((e >> 10) & 31));
+    }
   }
+  if (!D.sm) __threadfence_block();
   const i32 first = __shfl_sync(FULL, v, 0), last = __shfl_sync(FULL, v, (len - 1) & 31);
   if (len > 0) {
     const i64 w0 = (i64)((first - row_base) >> 5), w1 = (i64)((last - row_base) >> 5);
@@ -488,37 +517,131 @@ __device__ void dense_flip_regs(DenseCol& D, i32 v, int len, i32 row_base) {
   __syncwarp();
 }
 
+// Calls f(block) (warp-uniform) for every block of 32 data words in [b0, b1]
+// whose summary bit is set, in ascending order; f returns false to stop.
+template <typename F>
+__device__ __forceinline__ void for_each_block(const DenseCol& D, i64 b0, i64 b1, F&& f) {
+  const int lane = threadIdx.x & 31;
+  for (i64 s0 = (b0 >> 5); s0 <= (b1 >> 5); s0 += 32) {
+    const i64 sw = s0 + lane;
+    u32 m = sw <= (b1 >> 5) ? sm_ld32(D.sum + sw) : 0u;
+    if (sw == (b0 >> 5)) m &= ~0u << (b0 & 31);
+    if (sw == (b1 >> 5) && (b1 & 31) != 31) m &= (2u << (b1 & 31)) - 1u;
+    u32 lanes = __ballot_sync(FULL, m != 0);
+    while (lanes) {
+      const int l = __ffs(lanes) - 1;
+      lanes &= lanes - 1;
+      u32 bits = __shfl_sync(FULL, m, l);
+      while (bits) {
+        const int b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (!f(((s0 + l) << 5) + b)) return;
+      }
+    }
+  }
+}
+
+// for_each_block in batches: g(blocks, nb) with up to eight blocks at a time
+// (warp-uniform, ascending), so that their loads can be in flight together
+template <typename G>
+__device__ __forceinline__ void for_each_block8(const DenseCol& D, i64 b0, i64 b1, G&& g) {
+  i64 buf[8];
+  int nb = 0;
+  for_each_block(D, b0, b1, [&](i64 b) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (q == nb) buf[q] = b;
+    if (++nb == 8) {
+      g(buf, 8);
+      nb = 0;
+    }
+    return true;
+  });
+  if (nb) g(buf, nb);
+}
+
 // set bits of the bitmap (all at or after the pivot's word)
 __device__ int dense_count(const DenseCol& D, i32 row_base) {
   const int lane = threadIdx.x & 31;
   int c = 0;
-  for (i64 w = (i64)((D.piv - row_base) >> 5) + lane; w <= D.hi; w += 32) c += __popc(dense_word(D, w));
+  const i64 w0 = (i64)((D.piv - row_base) >> 5);
+  if (D.sum) {
+    for_each_block8(D, w0 >> 5, D.hi >> 5, [&](const i64* bs, int nb) {
+      u32 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const i64 w = (bs[q] << 5) + lane;
+        v[q] = (q < nb && w >= w0 && w <= D.hi) ? __ldcg(D.bits + w) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) c += __popc(v[q]);
+    });
+    return __reduce_add_sync(FULL, c);
+  }
+  for (i64 w = w0 + lane; w <= D.hi; w += 32) c += __popc(dense_word(D, w));
   return __reduce_add_sync(FULL, c);
 }
 
-__device__ int dense_flip(DenseCol& D, const i32* src, bool srcg, int len, i32 row_base) {
-  const int lane = threadIdx.x & 31;
-  int delta = 0;
-  for (int i = lane; i < len; i += 32) {
-    const i32 e = (srcg ? __ldcg(src + i) : src[i]) - row_base;
-    const u32 b = 1u << (e & 31);
-    const u32 old = dense_xor(D, e >> 5, b);
-    delta += (old & b) ? -1 : 1;
+// one entry's flip: the bitmap bit, and the summary bit of its block
+__device__ __forceinline__ void dense_flip1(const DenseCol& D, i32 e) {
+  const u32 b = 1u << (e & 31);
+  if (D.sm) {
+    sm_red_xor32(D.bits + (e >> 5), b);
+  } else {
+    gl_red_xor32(D.bits + (e >> 5), b);
+    if (D.sum) sm_red_or32(D.sum + (e >> 15), 1u << ((e >> 10) & 31));
   }
-  delta = __reduce_add_sync(FULL, delta);
+}
+
+// flips the sorted entries src[0..len) (global ranks) and widens the touched
+// range. Flips are fire-and-forget reductions (nothing waits for the old
+// words; the set-bit count is taken when the column is published), with eight
+// source loads per lane in flight: an added column can hold 10^5 entries.
+__device__ void dense_flip(DenseCol& D, const i32* src, bool srcg, int len, i32 row_base) {
+  const int lane = threadIdx.x & 31;
+  int i = lane;
+  for (; i + 224 < len; i += 256) {
+    i32 e[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) e[q] = (srcg ? __ldcg(src + i + 32 * q) : src[i + 32 * q]) - row_base;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) dense_flip1(D, e[q]);
+  }
+  for (; i < len; i += 32) dense_flip1(D, (srcg ? __ldcg(src + i) : src[i]) - row_base);
   if (len > 0) {
     const i64 w0 = (i64)(((srcg ? __ldcg(src) : src[0]) - row_base) >> 5);
     const i64 w1 = (i64)(((srcg ? __ldcg(src + len - 1) : src[len - 1]) - row_base) >> 5);
     D.lo = D.hi < D.lo ? w0 : min(D.lo, w0);
     D.hi = max(D.hi, w1);
   }
+  // the flips are visible to the warp's later loads of the bitmap
+  if (!D.sm) __threadfence_block();
   __syncwarp();
-  return delta;
 }
 
 // first set bit at or after word `from` (global rank), -1 if none
 __device__ i32 dense_first(const DenseCol& D, i64 from, i32 row_base) {
   const int lane = threadIdx.x & 31;
+  if (D.sum) {
+    i32 found = -1;
+    for_each_block(D, from >> 5, D.hi >> 5, [&](i64 b) {
+      const i64 w = (b << 5) + lane;
+      const u32 v = (w >= from && w <= D.hi) ? __ldcg(D.bits + w) : 0u;
+      const u32 m = __ballot_sync(FULL, v != 0);
+      if (m) {
+        const int f = __ffs(m) - 1;
+        const u32 vw = __shfl_sync(FULL, v, f);
+        found = (i32)((((b << 5) + f) << 5) + (__ffs(vw) - 1)) + row_base;
+        return false;
+      }
+      // an empty block (every bit it held was flipped away): drop its summary
+      // bit, unless part of it lies before `from` (those words were not read)
+      if ((b << 5) >= from && lane == 0) sm_red_and32(D.sum + (b >> 5), ~(1u << (b & 31)));
+      __syncwarp();
+      return true;
+    });
+    return found;
+  }
   for (i64 w0 = from; w0 <= D.hi; w0 += 32) {
     const i64 w = w0 + lane;
     const u32 v = w <= D.hi ? dense_word(D, w) : 0u;
@@ -536,7 +659,39 @@ __device__ i32 dense_first(const DenseCol& D, i64 from, i32 row_base) {
 __device__ void dense_to_list(const DenseCol& D, i32 row_base, i32* out) {
   const int lane = threadIdx.x & 31;
   int pos = 0;
-  for (i64 w0 = (i64)((D.piv - row_base) >> 5); w0 <= D.hi; w0 += 32) {
+  const i64 wp = (i64)((D.piv - row_base) >> 5);
+  if (D.sum) {
+    for_each_block8(D, wp >> 5, D.hi >> 5, [&](const i64* bs, int nb) {
+      u32 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const i64 w = (bs[q] << 5) + lane;
+        v[q] = (q < nb && w >= wp && w <= D.hi) ? __ldcg(D.bits + w) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (q >= nb) break;
+        const i64 w = (bs[q] << 5) + lane;
+        u32 x = v[q];
+        const int c = __popc(x);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(FULL, incl, o);
+          if (lane >= o) incl += t;
+        }
+        int at = pos + incl - c;
+        while (x) {
+          out[at++] = (i32)((w << 5) + (__ffs(x) - 1)) + row_base;
+          x &= x - 1;
+        }
+        pos += __shfl_sync(FULL, incl, 31);
+      }
+    });
+    __syncwarp();
+    return;
+  }
+  for (i64 w0 = wp; w0 <= D.hi; w0 += 32) {
     const i64 w = w0 + lane;
     u32 v = w <= D.hi ? dense_word(D, w) : 0u;
     const int c = __popc(v);
@@ -556,8 +711,27 @@ __device__ void dense_to_list(const DenseCol& D, i32 row_base, i32* out) {
   __syncwarp();
 }
 
+// zeroes the summary words of blocks [b0, b1]
+__device__ void dense_sum_zero(DenseCol& D, i64 b0, i64 b1) {
+  const int lane = threadIdx.x & 31;
+  for (i64 sw = (b0 >> 5) + lane; sw <= (b1 >> 5); sw += 32) sm_st32(D.sum + sw, 0u);
+  __syncwarp();
+}
+
 __device__ void dense_clear(DenseCol& D, i64 lo, i64 hi) {
   const int lane = threadIdx.x & 31;
+  if (D.sum && hi >= lo) {  // only the blocks that may hold set bits
+    for_each_block(D, lo >> 5, hi >> 5, [&](i64 b) {
+      __stcg(D.bits + (b << 5) + lane, 0u);
+      return true;
+    });
+    __syncwarp();
+    dense_sum_zero(D, lo >> 5, hi >> 5);
+    D.lo = 0;
+    D.hi = -1;
+    D.piv = -1;
+    return;
+  }
   if (D.sm)
     for (i64 w = lo + lane; w <= hi; w += 32) sm_st32(D.bits + w, 0u);
   else
@@ -595,7 +769,11 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
     D.sm = true;
   } else if (dense_ok) {
     D.bits = dense_bits + (size_t)(blockIdx.x * RD_WARPS + w) * (size_t)dense_words;
+    // the summary needs one bit per 32 data words; a slot's word count is
+    // bounded by the 1 GiB of slots, far below RD_SUM_WORDS * 1024 words
+    if ((dense_words + 1023) / 1024 <= RD_SUM_WORDS) D.sum = reinterpret_cast<u32*>(sBw);
   }
+  const i64 sum_blocks = (dwords + 31) / 32;
   for (;;) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&ctl->next, RD_FETCH);
@@ -617,12 +795,21 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
     u64 wrec = 0;         // record offset of W when published
     bool dense = false;   // W is the bitmap D
     auto enter_dense = [&](const i32* src, bool srcg, int len) {
+      // the summary shares its buffer with the list form's added-column copy:
+      // zero it whenever a column becomes a bitmap
+      if (D.sum) dense_sum_zero(D, 0, sum_blocks - 1);
       if (!dense_ready) {
+        u32* keep = D.sum;
+        D.sum = nullptr;  // the first clear covers the whole slot (its content is unknown)
         dense_clear(D, 0, dwords - 1);
+        D.sum = keep;
         dense_ready = true;
       }
-      dense_flip(D, src, srcg, len, row_base);
       D.piv = len > 0 ? (srcg ? __ldcg(src) : src[0]) : -1;
+      // the column's entries stay within [first pivot, first pivot + span):
+      // the bitmap window starts at the first pivot's word
+      D.rb = len > 0 ? row_base + (((D.piv - row_base) >> 5) << 5) : row_base;
+      dense_flip(D, src, srcg, len, D.rb);
       dense = true;
     };
     auto leave_dense = [&]() {
@@ -672,12 +859,12 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
       if (!take && o < c) {
         // publish W as a record, then claim p
         if (!published) {
-          if (dense) k = dense_count(D, row_base);
+          if (dense) k = dense_count(D, D.rb);
           const unsigned long long at = pool_alloc(chunk_state, ctl, pool_cap, k + 1, chunk, status);
           if (at == ~0ull) break;
           if (lane == 0) pool[at] = k;
           if (dense)
-            dense_to_list(D, row_base, pool + at + 1);
+            dense_to_list(D, D.rb, pool + at + 1);
           else
             for (int i = lane; i < k; i += 32) pool[at + 1 + i] = wg ? __ldcg(W + i) : W[i];
           wrec = at;
@@ -701,10 +888,10 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
             // the bitmap holds the claimer's content: flip the displaced record into it
             const u64 at_d = old & OW_OFF;
             const int len_d = __ldcg(pool + at_d);
-            dense_flip(D, pool + at_d + 1, true, len_d, row_base);
+            dense_flip(D, pool + at_d + 1, true, len_d, D.rb);
             ++n_merges;
             published = false;
-            D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+            D.piv = dense_first(D, (i64)((p - D.rb) >> 5), D.rb);
             if (D.piv < 0) {  // the column vanished
               k = 0;
               leave_dense();
@@ -736,12 +923,12 @@ __global__ void __launch_bounds__(RD_NT, 1) k_reduce(i32 row_base, i64 K, const 
       if (dense) {
         // entries 0..30 of the added column are already in registers
         if (lb <= 31)
-          dense_flip_regs(D, bv, lb, row_base);
+          dense_flip_regs(D, bv, lb, D.rb);
         else
-          dense_flip(D, pool + at_o + 1, true, lb, row_base);
+          dense_flip(D, pool + at_o + 1, true, lb, D.rb);
         ++n_merges;
         published = false;
-        D.piv = dense_first(D, (i64)((p - row_base) >> 5), row_base);
+        D.piv = dense_first(D, (i64)((p - D.rb) >> 5), D.rb);
         if (D.piv < 0) {  // the column vanished
           k = 0;
           leave_dense();
@@ -869,31 +1056,40 @@ int reduce_blocks(i64 K) {
   return (int)std::max<i64>(1, std::min<i64>((K + RD_WARPS - 1) / RD_WARPS, (i64)sms * std::max(occ, 1)));
 }
 
+// A dense working column's bitmap starts at the word of its first pivot and
+// must hold every row its entries can reach: `span` rows (all R rows for a
+// single cloud; in a batch, the largest row range of one cloud, since a
+// column only ever meets rows of its own cloud), plus a word of alignment.
+i64 window_words(i64 span) { return (span + 31) / 32 + 2; }
+
 // words of the shared-memory bitmap each warp uses for every working column,
-// 0 when R rows do not fit one working buffer
-int sm_dense_words(i64 R) {
-  const i64 words = (R + 31) / 32 + 1;
+// 0 when the window does not fit one working buffer
+int sm_dense_words(i64 span) {
+  const i64 words = window_words(span);
   return words <= RD_CAP ? (int)words : 0;
 }
 
-// dense working-column slots in global memory (rows beyond the shared bitmap):
-// one bitmap of R bits per warp of the grid, when they fit in 1 GiB (else long
+// dense working-column slots in global memory (windows beyond the shared
+// bitmap): one window per warp of the grid, when they fit in 1 GiB (else long
 // columns stay sorted lists in the pool)
-i64 dense_words(i64 K, i64 R) {
-  if (sm_dense_words(R)) return 0;
-  const i64 words = (R + 31) / 32 + 1;
+i64 dense_words(i64 K, i64 span) {
+  if (sm_dense_words(span)) return 0;
+  const i64 words = window_words(span);
   const i64 warps = (i64)reduce_blocks(K) * RD_WARPS;
   return words * warps * 4 <= (i64(1) << 30) ? words : 0;
 }
 
-extern "C" size_t ph_reduce_workspace_bytes(int64_t K, int64_t R) {
-  const i64 dw = K > 0 ? dense_words(K, R) : 0;
+inline i64 span_or_all(i64 R, i64 span) { return span > 0 && span < R ? span : R; }
+
+extern "C" size_t ph_reduce_workspace_bytes(int64_t K, int64_t R, int64_t span) {
+  span = span_or_all(R, span);
+  const i64 dw = K > 0 ? dense_words(K, span) : 0;
   return Carve::need((size_t)R * 8) + Carve::need((size_t)K * 8) + Carve::need(sizeof(RedCtl)) +
          (dw ? Carve::need((size_t)dw * 4 * reduce_blocks(K) * RD_WARPS) : 0);
 }
 
 extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,
-                         int64_t R, int32_t row_base, const uint8_t* skip, const int32_t* row_cmf,
+                         int64_t R, int32_t row_base, int64_t span, const uint8_t* skip, const int32_t* row_cmf,
                          int32_t* col_state, int32_t* col_piv, int32_t* pool, int64_t pool_cap,
                          int64_t* d_info, int* d_status, void* workspace, size_t workspace_bytes,
                          void* stream) {
@@ -920,14 +1116,15 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
     return PH_ERR_CUDA;
   }
   const int blocks = reduce_blocks(K);
-  const i64 dw = dense_words(K, R);
+  span = span_or_all(R, span);
+  const i64 dw = dense_words(K, span);
   u32* dense = dw ? c.take<u32>(dw * (i64)blocks * RD_WARPS) : nullptr;
   if (dw && !dense) return PH_ERR_ARG;
   // pool chunk per warp: small enough that the chunks of all warps fit a quarter of the pool
   const int chunk = (int)std::max<i64>(64, std::min<i64>(2048, pool_cap / (4 * (i64)blocks * RD_WARPS)));
   ph::count_launch();
   ph::launch_pdl(k_reduce, dim3(blocks), dim3(RD_NT), RD_SMEM, s, row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
-                                          1 << 24, dense, dw, sm_dense_words(R));
+                                          1 << 24, dense, dw, sm_dense_words(span));
   ph::count_launch();
   ph::launch_pdl(k_finish_cols, dim3(grid_for(K)), dim3(256), 0, s, K, col_state, col_piv, ctl, d_info);
   if (R > 0) {

@@ -61,6 +61,11 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
     const int l0 = a_short ? sb : sa, l1 = a_short ? eb : ea;
     int ntri = 0, ncof = 0;
     i64 out = EMIT ? tri_off[m] : 0;
+    // the emit pass writes only inside the edge's allotment [tri_off[m],
+    // tri_off[m + 1]): an edge allotted nothing (a batch can clear the
+    // triangles of some clouds after the count) is skipped
+    const i64 oend = EMIT ? tri_off[m + 1] : 0;
+    if (EMIT && oend <= out) continue;
     for (int base = s0; base < s1; base += 32) {
       const int p = base + lane;
       bool common = false, valid = false;
@@ -77,7 +82,7 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
       }
       const u32 cb = __ballot_sync(FULL, common);
       const u32 vb = __ballot_sync(FULL, valid);
-      if (EMIT && valid) {
+      if (EMIT && valid && out + __popc(vb & lt) < oend) {
         const i64 o = out + __popc(vb & lt);
         tm[o] = (i32)m;
         tw[o] = w;
@@ -165,6 +170,7 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
     const i64 t0 = tri_off[m], t1 = tri_off[m + 1];
     const int nw = (enable && !enable[m]) ? 0 : (int)(t1 - t0);
     i64 out = EMIT ? tet_off[m] : 0;
+    const i64 oend = EMIT ? tet_off[m + 1] : 0;  // writes stay inside the edge's allotment
     int cnt = 0;
     for (int i = 0; i + 1 < nw; ++i) {
       const i32 p = tw[t0 + i];
@@ -182,7 +188,7 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
           }
         }
         const u32 vb = __ballot_sync(FULL, valid);
-        if (EMIT && valid) {
+        if (EMIT && valid && out + __popc(vb & lt) < oend) {
           const i64 o = out + __popc(vb & lt);
           qm[o] = (i32)m;
           qf[4 * o + 0] = (i32)(t0 + i);

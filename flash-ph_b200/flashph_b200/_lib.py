@@ -59,6 +59,14 @@ _SIGS = {
     "ph_result_copy_all": (ctypes.c_int, [P, P, I32, P]),
     "ph_set_dependent_launch": (None, [I32]),
     "ph_result_free": (None, [P]),
+    "ph_rips_persistence_batch": (ctypes.c_int, [P, P, P, P, P, I32, I64, I64, I32, I64,
+                                                 ctypes.POINTER(ctypes.c_void_p), P]),
+    "ph_batch_result_status": (I32, [P, I32]),
+    "ph_batch_result_message": (ctypes.c_char_p, [P, I32]),
+    "ph_batch_result_stat": (I64, [P, I32, I32]),
+    "ph_batch_result_offsets": (ctypes.c_int, [P, I32, P]),
+    "ph_batch_result_copy": (ctypes.c_int, [P, I32, P, I32, P]),
+    "ph_batch_result_free": (None, [P]),
     "ph_triangles_total_max_vertices": (I64, []),
     "ph_triangles_total": (ctypes.c_int, [P, P, I64, P, P, P]),
     "ph_edges_screened_workspace_bytes": (SZ, [I64, I32, I32]),
@@ -81,8 +89,8 @@ _SIGS = {
     "ph_cofacet_csr_workspace_bytes": (SZ, [I64, I32]),
     "ph_cofacet_csr": (ctypes.c_int, [P, P, P, P, I32, I64, I64, I32, P, P, P, SZ, P]),
     "ph_cof_max_face": (ctypes.c_int, [P, P, P, P, I32, I64, I32, P, P, P]),
-    "ph_reduce_workspace_bytes": (SZ, [I64, I64]),
-    "ph_reduce": (ctypes.c_int, [P, P, I64, I32, I64, I32, P, P, P, P, P, I64, P, P, P, SZ, P]),
+    "ph_reduce_workspace_bytes": (SZ, [I64, I64, I64]),
+    "ph_reduce": (ctypes.c_int, [P, P, I64, I32, I64, I32, I64, P, P, P, P, P, I64, P, P, P, SZ, P]),
     "ph_mark_pivots": (ctypes.c_int, [P, P, I64, I32, P, I64, P]),
     "ph_persistence_rows_workspace_bytes": (SZ, [I64]),
     "ph_persistence_rows": (ctypes.c_int, [P, P, I64, I32, P, P, P, P, P, P, SZ, P]),
@@ -109,9 +117,10 @@ def lib():
     """The loaded CUDA library (built on first use if missing)."""
     global _LIB
     if _LIB is None:
-        path = _build.LIB_PATH
-        if not os.path.exists(path):
-            path = _build.build()
+        # the library must be the build of the sources next to it (the entry
+        # points' argument lists above follow those sources): rebuilt when
+        # missing or when the sources' digest differs from its build stamp
+        path = _build.build()
         handle = ctypes.CDLL(path)
         for name, (res, args) in _SIGS.items():
             fn = getattr(handle, name)

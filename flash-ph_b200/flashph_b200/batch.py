@@ -1,29 +1,30 @@
 """Batching form: many point clouds of uneven n and d in one pipeline.
 
 A batch is the disjoint union of its clouds (vertex v of cloud c has global
-index vbase_c + v). Edge enumeration walks (cloud, 128x128 tile) work items
-from a segment table, the filtration sort orders every cloud's edges by its
-own packed key (local indices), and everything after it -- adjacency,
-forest, triangles, tetrahedra, cofacets, the lock-free reduction -- runs on
-global indices unchanged, because no simplex spans two clouds. Rows are cut
-per cloud at the end. Every cloud's diagrams equal those of a separate
-``rips_persistence`` call on it, bit for bit.
+index vbase_c + v). ``rips_persistence_batch`` runs it through one native
+library call per chunk (``ph_rips_persistence_batch``): edge enumeration
+walks (cloud, tile) work items from a segment table, the filtration sort
+orders every cloud's edges by its own packed key (local indices), and
+everything after it -- adjacency, forest, triangles, tetrahedra, cofacets,
+the lock-free reduction -- runs on global indices unchanged, because no
+simplex spans two clouds; the host waits four times per chunk, whatever the
+number of clouds. Rows are cut per cloud at the end. Every cloud's diagrams
+equal those of a separate ``rips_persistence`` call on it, bit for bit.
 
-Clouds are processed in chunks bounded by point and pair counts. Errors that
-the reference raises per call (validation, the triangle and tetrahedron
-caps) are returned per cloud as exception objects; they do not stop the
-batch.
+Clouds are processed in chunks bounded by points and pairs; a chunk whose
+simplices exceed the rank range or the per-chunk simplex budget is split by
+the exact per-cloud counts the library returns. Errors that the reference
+raises per call (validation, the triangle and tetrahedron caps) are
+returned per cloud as exception objects; they do not stop the batch.
 
-Clouds of at least ``NATIVE_MIN_POINTS`` points do not join the chunks: each
-runs as one native pipeline call (``ph_rips_persistence``), two at a time on
-worker streams. The union pipeline pays off where a call's fixed cost (about
-80 short kernels and four host waits) dominates, i.e. for small clouds; for
-larger ones the native call, whose stages are specialised to one cloud and
-chained on the device, is faster.
+``FLASHPH_BATCH=staged`` runs the same union stage by stage from Python
+(each stage its own library call), a cross-check of the native call.
 """
 from __future__ import annotations
 
+import ctypes
 import math
+import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
 from typing import Sequence
@@ -47,8 +48,14 @@ _CHUNK_POINTS = 1 << 18
 _CHUNK_PAIRS = 1 << 34
 _CHUNK_TRIANGLES = 1 << 28   # per chunk, keeps every global rank in int32
 _CHUNK_TETS = 1 << 28
-NATIVE_MIN_POINTS = 1024  # clouds this large run as native calls
+NATIVE_MIN_POINTS = 1024  # staged form only: clouds this large run as native single calls
 _NATIVE_WORKERS = 2
+# native batch chunks: points, candidate pairs and simplices (triangles, plus
+# tetrahedra for H2) per library call
+_BATCH_POINTS = 1 << 20
+_BATCH_PAIRS = 1 << 36
+_BATCH_SIMPLICES = 1 << 27
+_EDGE_MODES = {"auto": 0, "on": 1, "off": 2}
 
 
 # Worker streams are kept for the life of the process and reused (by the
@@ -346,11 +353,11 @@ class _CapExceeded(Exception):
         self.errors = errors
 
 
-def _chunks(order, sizes):
+def _chunks(order, sizes, max_points=_CHUNK_POINTS, max_pairs=_CHUNK_PAIRS):
     chunk, pts, pairs = [], 0, 0
     for c in order:
         n = sizes[c]
-        if chunk and (pts + n > _CHUNK_POINTS or pairs + n * n // 2 > _CHUNK_PAIRS):
+        if chunk and (pts + n > max_points or pairs + n * n // 2 > max_pairs):
             yield chunk
             chunk, pts, pairs = [], 0, 0
         chunk.append(c)
@@ -358,6 +365,101 @@ def _chunks(order, sizes):
         pairs += n * n // 2
     if chunk:
         yield chunk
+
+
+class _Split(Exception):
+    """The chunk is over the rank range or the simplex budget; per-cloud
+    simplex counts (triangles + tetrahedra where counted) come with it."""
+
+    def __init__(self, counts: list[int], edges: list[int]):
+        super().__init__("split")
+        self.counts = counts
+        self.edges = edges
+
+
+def _native_chunk(pts: list[Tensor], ts: list[float], dims: list[int], device, max_triangles: int,
+                  max_tetrahedra: int) -> list:
+    """Diagrams (or the reference's ValueError) of every cloud of a chunk,
+    from one ph_rips_persistence_batch call; raises _Split when the library
+    asks for a smaller chunk."""
+    lib = L.lib()
+    k = len(pts)
+    ptrs = (ctypes.c_void_p * k)(*[p.data_ptr() for p in pts])
+    n = np.array([p.shape[0] for p in pts], dtype=np.int64)
+    d = np.array([p.shape[1] for p in pts], dtype=np.int32)
+    t = np.array(ts, dtype=np.float64)
+    md = np.array(dims, dtype=np.int32)
+    mode = _EDGE_MODES.get(os.environ.get("FLASHPH_EDGE_SCREEN", "auto").lower(), 0)
+    s = L.stream_handle(device)
+    res = ctypes.c_void_p()
+    rc = lib.ph_rips_persistence_batch(ptrs, n.ctypes.data, d.ctypes.data, t.ctypes.data, md.ctypes.data, k,
+                                       max_triangles, max_tetrahedra, mode, _BATCH_SIMPLICES, ctypes.byref(res), s)
+    if rc == 3 and res.value:  # PH_ERR_CAPACITY: split by the exact counts
+        try:
+            tri = [max(0, int(lib.ph_batch_result_stat(res, c, 1))) for c in range(k)]
+            tet = [max(0, int(lib.ph_batch_result_stat(res, c, 2))) for c in range(k)]
+            edg = [max(0, int(lib.ph_batch_result_stat(res, c, 0))) for c in range(k)]
+        finally:
+            lib.ph_batch_result_free(res)
+        raise _Split([a + b for a, b in zip(tri, tet)], edg)
+    if rc != L.PH_OK:
+        raise L.PHError("ph_rips_persistence_batch", rc, lib.ph_last_error().decode(errors="replace"))
+    try:
+        top = max(dims)
+        bufs, offs = [], []
+        for dim in range(top + 1):
+            off = np.zeros(k + 1, dtype=np.int64)
+            L.call("ph_batch_result_offsets", res, dim, off.ctypes.data)
+            buf = torch.empty(max(int(off[-1]), 1), 2, dtype=torch.float32, device=device)
+            L.call("ph_batch_result_copy", res, dim, buf.data_ptr(), 0, s)
+            bufs.append(buf)
+            offs.append(off)
+        out = []
+        for c in range(k):
+            if int(lib.ph_batch_result_status(res, c)) != L.PH_OK:
+                out.append(ValueError(lib.ph_batch_result_message(res, c).decode(errors="replace")))
+                continue
+            out.append([bufs[dim][int(offs[dim][c]):int(offs[dim][c + 1])] for dim in range(dims[c] + 1)])
+    finally:
+        lib.ph_batch_result_free(res)
+    return out
+
+
+def _repack(chunk: list[int], counts: list[int], edges: list[int]) -> list[list[int]]:
+    """A split chunk packed again by its exact per-cloud simplex counts."""
+    parts, cur, simp, ed = [], [], 0, 0
+    for c, q, e in zip(chunk, counts, edges):
+        if cur and (simp + q > _BATCH_SIMPLICES or ed + e + 3 * (simp + q) >= (1 << 31) - (1 << 24)):
+            parts.append(cur)
+            cur, simp, ed = [], 0, 0
+        cur.append(c)
+        simp += q
+        ed += e
+    if cur:
+        parts.append(cur)
+    if len(parts) == 1 and len(chunk) > 1:  # the counts fit after all (the budget counts H2 too): halve
+        h = len(chunk) // 2
+        parts = [chunk[:h], chunk[h:]]
+    return parts
+
+
+def _to_device_all(pts: list[Tensor], device) -> list[Tensor]:
+    """float32 contiguous device copies of the clouds; host clouds go over in
+    one pinned copy."""
+    host = [i for i, p in enumerate(pts) if p.device.type != "cuda"]
+    out = list(pts)
+    if host:
+        flat = torch.cat([pts[i].reshape(-1).float() for i in host])
+        dev = flat.pin_memory().to(device, non_blocking=True) if flat.numel() else flat.to(device)
+        at = 0
+        for i in host:
+            m = pts[i].numel()
+            out[i] = dev[at:at + m].view(pts[i].shape[0], pts[i].shape[1])
+            at += m
+    for i, p in enumerate(out):
+        if i not in host:
+            out[i] = p.to(device).float().contiguous()
+    return out
 
 
 def rips_persistence_batch(
@@ -401,6 +503,31 @@ def rips_persistence_batch(
             results[c] = _trivial(t.shape[0], ds[c], device)
         else:
             todo.append(c)
+    if os.environ.get("FLASHPH_BATCH", "native") == "staged":
+        _staged_batch(pts, ts, ds, todo, results, device, max_triangles, max_tetrahedra)
+        return results
+    dev_pts = _to_device_all([pts[c] for c in todo], device)
+    dpts = dict(zip(todo, dev_pts))
+    sizes = {c: int(pts[c].shape[0]) for c in todo}
+    work = list(_chunks(todo, sizes, _BATCH_POINTS, _BATCH_PAIRS))
+    while work:
+        chunk = work.pop(0)
+        try:
+            res = _native_chunk([dpts[c] for c in chunk], [ts[c] for c in chunk], [ds[c] for c in chunk], device,
+                                max_triangles, max_tetrahedra)
+        except _Split as sp:
+            if len(chunk) == 1:  # one cloud beyond the int32 rank range
+                results[chunk[0]] = ValueError("Simplex count exceeds the int32 rank range")
+                continue
+            work[:0] = _repack(chunk, sp.counts, sp.edges)
+            continue
+        for c, r in zip(chunk, res):
+            results[c] = r
+    return results
+
+
+def _staged_batch(pts, ts, ds, todo, results, device, max_triangles, max_tetrahedra):
+    """The union stage by stage from Python (cross-check of the native batch)."""
     native = [c for c in todo if int(pts[c].shape[0]) >= NATIVE_MIN_POINTS]
     if native:
         done = _run_native([(c, pts[c], ts[c], ds[c]) for c in native], device, max_triangles, max_tetrahedra)
@@ -428,7 +555,6 @@ def rips_persistence_batch(
             else:
                 h = len(chunk) // 2
                 work[:0] = [chunk[:h], chunk[h:]]
-    return results
 
 
 def auto_threshold_batch(clouds: Sequence, k: int = 20, percentile: float = 95.0) -> list[float]:

@@ -103,17 +103,18 @@ def cof_max_face(S: int, k: int, face_base: int, skip: Tensor, faces_aos=None, f
 
 
 def reduce(cof_off: Tensor, cof_data: Tensor, K: int, col_base: int, R: int, row_base: int,
-           skip: Tensor | None, cmf: Tensor, pool_cap: int) -> Reduction:
-    """Enqueue the reduction (no host synchronisation)."""
+           skip: Tensor | None, cmf: Tensor, pool_cap: int, span: int = 0) -> Reduction:
+    """Enqueue the reduction (no host synchronisation). ``span``: the most
+    rows one column's entries can span (0: all R rows)."""
     dev = cof_off.device
     state = torch.empty(K, dtype=torch.int32, device=dev)
     piv = torch.empty(K, dtype=torch.int32, device=dev)
     info = torch.zeros(4, dtype=torch.int64, device=dev)
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     pool = torch.empty(max(pool_cap, 1), dtype=torch.int32, device=dev)
-    nb = L.query("ph_reduce_workspace_bytes", K, R)
+    nb = L.query("ph_reduce_workspace_bytes", K, R, span)
     ws = L.workspace(nb, dev)
-    L.call("ph_reduce", cof_off.data_ptr(), L.ptr(cof_data), K, col_base, R, row_base, L.ptr(skip),
+    L.call("ph_reduce", cof_off.data_ptr(), L.ptr(cof_data), K, col_base, R, row_base, span, L.ptr(skip),
            L.ptr(cmf), L.ptr(state), L.ptr(piv), pool.data_ptr(), pool_cap, info.data_ptr(),
            status.data_ptr(), ws.data_ptr(), nb, L.stream_handle(dev))
     return Reduction(state, piv, info, status)

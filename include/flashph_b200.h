@@ -275,12 +275,16 @@ int ph_cof_max_face(const int32_t* faces_aos, const int32_t* f0, const int32_t* 
  * col_state[c]: 0 skipped, 1 apparent, 2 reduced to a pivot, 3 essential.
  * col_piv[c]: pivot global rank (states 1 and 2) or -1.
  * pool: scratch for reduced columns, pool_cap int32 entries.
+ * span: the most rows one column's entries can span (its rows all lie in a
+ * range of span consecutive ranks: in a batch, the largest row count of one
+ * cloud); 0 or R for a single cloud. Working columns that become bitmaps
+ * need only that many bits.
  * d_info (int64 x 4, device): [residual columns, column additions, pool
  * entries used, takeovers].
  * d_status: PH_ERR_POOL or PH_ERR_ITER_LIMIT on failure. */
-size_t ph_reduce_workspace_bytes(int64_t K, int64_t R);
+size_t ph_reduce_workspace_bytes(int64_t K, int64_t R, int64_t span);
 int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_t K, int32_t col_base,
-              int64_t R, int32_t row_base, const uint8_t* skip, const int32_t* row_cmf,
+              int64_t R, int32_t row_base, int64_t span, const uint8_t* skip, const int32_t* row_cmf,
               int32_t* col_state, int32_t* col_piv, int32_t* pool, int64_t pool_cap,
               int64_t* d_info, int* d_status, void* workspace, size_t workspace_bytes,
               void* stream);
@@ -337,6 +341,42 @@ int ph_result_copy_all(const ph_result* result, float* dst, int32_t to_host, voi
 /* releases the diagrams and the run's intermediate buffers (stream-ordered, on
  * the stream of the run, after every copy queued before it) */
 void ph_result_free(ph_result* result);
+
+/* ---- the whole call for a batch of clouds ------------------------------------ */
+
+/* rips_persistence for every cloud of a batch in one call (the reference has
+ * no batched API; this replaces one persistence.py:77-215 call per cloud):
+ * points[c] (device, n[c] x d[c] float32, n[c] >= 2), max_edge_length[c],
+ * max_dim[c] (0..2; H2 needs n[c] < 65536), the reference's per-call limits,
+ * edge_mode as in ph_rips_persistence (0: the tensor-core screen when the
+ * largest d is in [8, 252]). The clouds run as one disjoint union on
+ * `stream`; the host waits four times whatever their number. A cloud over a
+ * limit gets status PH_ERR_LIMIT and the reference's ValueError text
+ * (ph_batch_result_status / _message); the others are unaffected, and every
+ * cloud's diagrams equal ph_rips_persistence on it alone, bit for bit.
+ * Returns PH_ERR_CAPACITY, with *out set and the per-cloud counts filled,
+ * when the union's simplices exceed the int32 rank range or, for more than
+ * one cloud, max_batch_simplices (triangles, then triangles + tetrahedra;
+ * 0: no budget): the caller splits the batch (ph_batch_result_stat gives each
+ * cloud's edges and triangles) and frees *out. */
+typedef struct ph_batch_result ph_batch_result;
+int ph_rips_persistence_batch(const float* const* points, const int64_t* n, const int32_t* d,
+                              const double* max_edge_length, const int32_t* max_dim, int32_t nclouds,
+                              int64_t max_triangles, int64_t max_tetrahedra, int32_t edge_mode,
+                              int64_t max_batch_simplices, ph_batch_result** out, void* stream);
+/* PH_OK or PH_ERR_LIMIT for cloud c, and the limit's message ("" if none) */
+int32_t ph_batch_result_status(const ph_batch_result* result, int32_t cloud);
+const char* ph_batch_result_message(const ph_batch_result* result, int32_t cloud);
+/* per-cloud counts: k = 0 edges, 1 triangles, 2 tetrahedra (-1: not counted) */
+int64_t ph_batch_result_stat(const ph_batch_result* result, int32_t cloud, int32_t k);
+/* nclouds + 1 row offsets of diagram dim in the batch's rows of that dim
+ * (cloud c's rows are [out[c], out[c+1]); all zero when no cloud has dim) */
+int ph_batch_result_offsets(const ph_batch_result* result, int32_t dim, int64_t* out);
+/* copies all rows of diagram dim (out[nclouds] x 2 float32) to dst, device or
+ * host memory, on any stream (the run's frees wait for the copy) */
+int ph_batch_result_copy(const ph_batch_result* result, int32_t dim, float* dst, int32_t to_host, void* stream);
+/* releases the rows and the run's buffers (stream-ordered on the run's stream) */
+void ph_batch_result_free(ph_batch_result* result);
 
 /* ---- batches of clouds ---------------------------------------------------- */
 /* The reference has no batched API; each entry below does, for every cloud of

@@ -51,6 +51,16 @@ def _load():
         lib.oracle_collapse_slots.restype = ctypes.c_void_p
         lib.oracle_collapse_slots.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                               ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        lib.oracle_edge_dsq.restype = None
+        lib.oracle_edge_dsq.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_void_p]
+        lib.oracle_row_edges.restype = ctypes.c_void_p
+        lib.oracle_row_edges.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int]
+        lib.oracle_run_edges.restype = ctypes.c_void_p
+        lib.oracle_run_edges.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                         ctypes.c_int64, ctypes.c_int]
         lib.oracle_error.restype = ctypes.c_char_p
         lib.oracle_error.argtypes = [ctypes.c_void_p]
         lib.oracle_free.argtypes = [ctypes.c_void_p]
@@ -124,6 +134,43 @@ def collapse_slots(points, max_edge_length: float, fused: bool = True, nthreads:
     n, d = pts.shape
     h = lib.oracle_collapse_slots(pts.ctypes.data if n else None, n, d, float(max_edge_length),
                                   int(bool(fused)), int(nthreads))
+    return _collect(lib, h)
+
+
+def edge_dsq(points, edge_i, edge_j, fused: bool = True, nthreads: int = 0) -> np.ndarray:
+    """dist^2 of the given pairs with the edge kernel's chain (edge_kernel.py:111-123)."""
+    lib = _load()
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+    ei = np.ascontiguousarray(edge_i, dtype=np.int32)
+    ej = np.ascontiguousarray(edge_j, dtype=np.int32)
+    out = np.empty(ei.shape[0], dtype=np.float32)
+    if ei.shape[0]:
+        lib.oracle_edge_dsq(pts.ctypes.data, pts.shape[0], pts.shape[1], ei.ctypes.data, ej.ctypes.data,
+                            ei.shape[0], int(bool(fused)), int(nthreads), out.ctypes.data)
+    return out
+
+
+def row_edges(points, max_edge_length: float, rows, fused: bool = True, nthreads: int = 0) -> dict:
+    """The edges (min, max) incident to each listed row, j ascending per row
+    (keys edge_i, edge_j, edge_dsq): the rows' slice of the edge set."""
+    lib = _load()
+    pts = np.ascontiguousarray(np.asarray(points, dtype=np.float32))
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    h = lib.oracle_row_edges(pts.ctypes.data, pts.shape[0], pts.shape[1], float(max_edge_length),
+                             r.ctypes.data, r.shape[0], int(bool(fused)), int(nthreads))
+    return _collect(lib, h)
+
+
+def run_edges(edge_i, edge_j, edge_dsq, n: int, max_dim: int = 1) -> dict:
+    """The oracle pipeline from a given edge list in any order: emission order
+    restored from (i, j), packed-key stable sort, H0..H2 (keys as ``run``)."""
+    lib = _load()
+    ei = np.ascontiguousarray(edge_i, dtype=np.int32)
+    ej = np.ascontiguousarray(edge_j, dtype=np.int32)
+    ed = np.ascontiguousarray(edge_dsq, dtype=np.float32)
+    E = ei.shape[0]
+    h = lib.oracle_run_edges(ei.ctypes.data if E else None, ej.ctypes.data if E else None,
+                             ed.ctypes.data if E else None, E, int(n), int(max_dim))
     return _collect(lib, h)
 
 

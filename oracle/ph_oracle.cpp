@@ -906,6 +906,22 @@ bool collapse_edges_relaxed(i64 n, const std::vector<i32>& ei, const std::vector
   return true;
 }
 
+// [lo, hi) ranges of 0..count over nthreads threads (all cores when 0)
+template <typename F>
+void parallel_ranges(i64 count, int nthreads, F&& body) {
+  int nt = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
+  if (nt > count) nt = (int)std::max<i64>(1, count);
+  const i64 step = (count + nt - 1) / std::max(nt, 1);
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) {
+    const i64 lo = t * step, hi = std::min<i64>(count, lo + step);
+    if (lo < hi) pool.emplace_back([&body, lo, hi]() { body(lo, hi); });
+  }
+  body(0, std::min<i64>(count, step));
+  for (auto& th : pool) th.join();
+}
+__attribute__((target("fma"))) inline float fma_hw(float a, float b, float c) { return __builtin_fmaf(a, b, c); }
+
 // H0 and, up to max_dim, H1 and H2 of the sorted filtration in R (edge ranks =
 // filtration order, filt = value per rank): persistence.py:160-215.
 void run_from_sorted(Result* R, i64 n, const std::vector<float>& filt, int max_dim, int stop_after) {
@@ -1041,6 +1057,116 @@ void* oracle_collapse_slots(const float* pts, int64_t n, int d, double max_edge_
                              R->collapse_rounds)) {
     R->error = "oracle_collapse_slots: n > 4096 or no edge ready";
   }
+  return R;
+}
+
+// dist^2 of given pairs (i, j) with the chain of enumerate_edges (fused or
+// not): the arithmetic of edge_kernel.py:111-123 for each pair, so that a
+// candidate edge list can be checked bit for bit without enumerating all
+// n(n-1)/2 pairs.
+void oracle_edge_dsq(const float* pts, int64_t n, int d, const int32_t* ei, const int32_t* ej, int64_t E,
+                     int fused, int nthreads, float* out) {
+  (void)n;
+  const bool hw_fma = __builtin_cpu_supports("fma");
+  auto body = [&](i64 lo, i64 hi) {
+    for (i64 e = lo; e < hi; ++e) {
+      const float* x = pts + (i64)ei[e] * d;
+      const float* y = pts + (i64)ej[e] * d;
+      float acc = 0.0f;
+      for (int k = 0; k < d; ++k) {
+        const float df = x[k] - y[k];
+        acc = fused ? (hw_fma ? fma_hw(df, df, acc) : __builtin_fmaf(df, df, acc)) : acc + df * df;
+      }
+      out[e] = acc;
+    }
+  };
+  parallel_ranges(E, nthreads, body);
+}
+
+// Every pair (r, j), j != r, of the rows r listed in `rows` with dist^2 below
+// the threshold (chain of enumerate_edges), written as edges (min, max) with
+// their dist^2, rows in the given order, j ascending: the rows' slice of the
+// edge set of edge_kernel.py:152 for a completeness check of a GPU edge list.
+void* oracle_row_edges(const float* pts, int64_t n, int d, double max_edge_length, const int32_t* rows,
+                       int64_t m, int fused, int nthreads) {
+  Result* R = new Result();
+  const float thr = oracle_threshold_sq(max_edge_length);
+  const bool hw_fma = __builtin_cpu_supports("fma");
+  std::vector<std::vector<i32>> vi(m), vj(m);
+  std::vector<std::vector<float>> vd(m);
+  auto body = [&](i64 lo, i64 hi) {
+    for (i64 q = lo; q < hi; ++q) {
+      const i64 r = rows[q];
+      const float* x = pts + r * d;
+      for (i64 j = 0; j < n; ++j) {
+        if (j == r) continue;
+        // the kernel's operand order: the lower index is the source row
+        const float* a = j < r ? pts + j * d : x;
+        const float* b = j < r ? x : pts + j * d;
+        float acc = 0.0f;
+        for (int k = 0; k < d; ++k) {
+          const float df = a[k] - b[k];
+          acc = fused ? (hw_fma ? fma_hw(df, df, acc) : __builtin_fmaf(df, df, acc)) : acc + df * df;
+        }
+        if (acc < thr) {
+          vi[q].push_back((i32)std::min<i64>(r, j));
+          vj[q].push_back((i32)std::max<i64>(r, j));
+          vd[q].push_back(acc);
+        }
+      }
+    }
+  };
+  parallel_ranges(m, nthreads, body);
+  for (i64 q = 0; q < m; ++q) {
+    R->edge_i.insert(R->edge_i.end(), vi[q].begin(), vi[q].end());
+    R->edge_j.insert(R->edge_j.end(), vj[q].begin(), vj[q].end());
+    R->edge_dsq.insert(R->edge_dsq.end(), vd[q].begin(), vd[q].end());
+  }
+  return R;
+}
+
+// The pipeline from a given edge list (any order): the edges are first put
+// in the reference kernel's emission order (32-point tiles (I, J), I <= J,
+// row-major over the flattened nb x nb grid, row-major inside a tile:
+// edge_kernel.py:134-149,208-210), then sorted by the packed key stably
+// (rips.py:30-50,188-202), then H0..H2 as oracle_run does. With the edge
+// set of edge_kernel.py this is oracle_run without the O(n^2 d) enumeration,
+// for checking large clouds whose edge list was checked separately.
+void* oracle_run_edges(const int32_t* ei, const int32_t* ej, const float* edsq, int64_t E, int64_t n,
+                       int max_dim) {
+  Result* R = new Result();
+  if (n <= 1) {
+    if (n == 1) {
+      R->h0 = {0.0f, INFINITY};
+      R->n_components = 1;
+    }
+    return R;
+  }
+  const i64 B = 32, nb = (n + B - 1) / B;
+  std::vector<u64> ek(E);
+  for (i64 e = 0; e < E; ++e) {
+    const i64 i = ei[e], j = ej[e];
+    if (!(0 <= i && i < j && j < n)) {
+      R->error = "oracle_run_edges: an edge is not (i, j) with 0 <= i < j < n";
+      return R;
+    }
+    ek[e] = ((u64)((i / B) * nb + j / B) << 10) | (u64)((i % B) * B + j % B);
+  }
+  std::vector<i64> perm(E);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::sort(perm.begin(), perm.end(), [&](i64 a, i64 b) { return ek[a] < ek[b]; });
+  R->edge_i.resize(E);
+  R->edge_j.resize(E);
+  R->edge_dsq.resize(E);
+  for (i64 k = 0; k < E; ++k) {
+    R->edge_i[k] = ei[perm[k]];
+    R->edge_j[k] = ej[perm[k]];
+    R->edge_dsq[k] = edsq[perm[k]];
+  }
+  sort_edges(R->edge_i, R->edge_j, R->edge_dsq);
+  std::vector<float> filt(E);
+  for (i64 e = 0; e < E; ++e) filt[e] = std::sqrt(R->edge_dsq[e]);
+  run_from_sorted(R, n, filt, max_dim, 0);
   return R;
 }
 

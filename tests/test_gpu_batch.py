@@ -125,3 +125,95 @@ def test_large_clouds_take_the_native_route_and_match_single_calls():
         for dim in range(md + 1):
             assert r[dim].device.type == "cuda"
             assert _same(r[dim], single[dim]), (p.shape, dim)
+
+
+def _mixed_clouds(seed=23):
+    """Clouds of every kind the batch must keep apart: H0-only, H1, H2, n = 2,
+    a cloud over the triangle limit, one over the tetrahedron limit, both edge
+    kernels' dimensions."""
+    rng = np.random.default_rng(seed)
+    clouds, ts, dims = [], [], []
+    for k in range(18):
+        n = int(rng.integers(2, 700))
+        d = int(rng.choice([2, 3, 8, 32]))
+        clouds.append(rng.standard_normal((n, d)).astype(np.float32))
+        ts.append(float({2: 0.6, 3: 0.9, 8: 2.6, 32: 6.8}[d]))
+        dims.append(int(rng.choice([0, 1, 2])))
+    clouds.append((rng.standard_normal((500, 3)) * 0.05).astype(np.float32))  # over max_triangles
+    ts.append(10.0)
+    dims.append(1)
+    clouds.append((rng.standard_normal((120, 4)) * 0.3).astype(np.float32))  # complete: C(120,4) > max_tetrahedra
+    ts.append(2.5)
+    dims.append(2)
+    return clouds, ts, dims
+
+
+def test_native_batch_equals_staged_batch_and_single_calls(monkeypatch):
+    """ph_rips_persistence_batch (one library call for the whole union)
+    against the stage-by-stage union and against single calls, bit for bit;
+    per-cloud limit errors carry the reference's texts."""
+    from flashph_b200 import rips_persistence
+    from flashph_b200.batch import rips_persistence_batch
+    clouds, ts, dims = _mixed_clouds()
+    native = rips_persistence_batch(clouds, ts, dims, max_triangles=2_000_000, max_tetrahedra=1_000_000)
+    monkeypatch.setenv("FLASHPH_BATCH", "staged")
+    staged = rips_persistence_batch(clouds, ts, dims, max_triangles=2_000_000, max_tetrahedra=1_000_000)
+    monkeypatch.delenv("FLASHPH_BATCH")
+    assert isinstance(native[-2], ValueError) and "max_triangles=2000000" in str(native[-2])
+    assert isinstance(native[-1], ValueError) and "max_tetrahedra=1000000" in str(native[-1])
+    for c, (p, t, md, a, b) in enumerate(zip(clouds, ts, dims, native, staged)):
+        if isinstance(a, Exception):
+            assert isinstance(b, ValueError) and str(a) == str(b), c
+            with pytest.raises(ValueError) as ex:
+                _single_with_limits(p, t, md)
+            assert str(ex.value) == str(a), c
+            continue
+        single = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=md)
+        assert len(a) == len(b) == md + 1, c
+        for dim in range(md + 1):
+            assert _same(a[dim], b[dim]) and _same(a[dim], single[dim]), (c, dim)
+
+
+def _single_with_limits(p, t, md):
+    """rips_persistence of one cloud with the limits of the batch above."""
+    from flashph_b200.persistence import _compute_native
+    x = torch.from_numpy(p).cuda()
+    return _compute_native(x, t, md, x.device, 2_000_000, 1_000_000)
+
+
+def test_batch_split_by_the_simplex_budget(monkeypatch):
+    """A budget small enough to split every chunk: the library reports the
+    per-cloud counts, the batch is packed again, results are unchanged."""
+    from flashph_b200 import batch as B
+    clouds, ts, dims = _mixed_clouds(seed=29)
+    whole = B.rips_persistence_batch(clouds, ts, dims, max_triangles=2_000_000, max_tetrahedra=1_000_000)
+    monkeypatch.setattr(B, "_BATCH_SIMPLICES", 30_000)
+    split = B.rips_persistence_batch(clouds, ts, dims, max_triangles=2_000_000, max_tetrahedra=1_000_000)
+    for a, b in zip(whole, split):
+        if isinstance(a, Exception):
+            assert str(a) == str(b)
+            continue
+        for x, y in zip(a, b):
+            assert _same(x, y)
+
+
+def test_union_of_dense_clouds_matches_single_calls():
+    """Dense clouds of the batching configuration (noisy rotated Clifford tori
+    and Gaussian clouds at the 95th percentile of 20-NN distances, 800-1900
+    points) in one union: several clouds with millions of triangle rows, whose
+    working-column bitmaps are windows of one cloud's row range. Each against
+    its single call, bit for bit."""
+    import bench
+    from flashph_b200 import rips_persistence
+    from flashph_b200.batch import auto_threshold_batch, rips_persistence_batch
+    rng = np.random.default_rng(31)
+    clouds = []
+    for k, (n, d) in enumerate([(1100, 8), (1900, 3), (800, 32), (1500, 8), (1300, 3)]):
+        clouds.append(rng.standard_normal((n, d)).astype(np.float32) if k % 2 == 0
+                      else bench.clifford_cloud(n, d, rng))
+    ts = auto_threshold_batch(clouds, k=20, percentile=95.0)
+    res = rips_persistence_batch(clouds, ts, 1)
+    for p, t, r in zip(clouds, ts, res):
+        single = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=1)
+        assert not isinstance(r, Exception), r
+        assert _same(r[0], single[0]) and _same(r[1], single[1])

@@ -260,3 +260,36 @@ def test_h2_with_list_columns_matches_oracle():
     assert _same_rows(got[0].cpu(), ref["h0"])
     assert _same_rows(got[1].cpu(), ref["h1"])
     assert _same_rows(sorted_rows(got[2].cpu().numpy()), sorted_rows(ref["h2"]))
+
+
+def test_dense_h1_with_ten_million_rows_matches_oracle():
+    """A batching-configuration-sized dense cloud (n = 1898, d = 8, t = 2.701:
+    202,737 edges, 9,776,543 triangle rows, working columns up to 127,972
+    entries): the global bitmaps span ~9.8M rows and are scanned through their
+    shared-memory summary (one bit per 1024 rows). Bit for bit against the
+    oracle."""
+    import oracle
+    from flashph_b200 import rips_persistence
+    p = np.random.default_rng(2).standard_normal((1898, 8)).astype(np.float32)
+    ref = oracle.run(p, 2.701, 1, fused=True)
+    assert ref["T"] > 9_000_000 and ref["col_max"] > 100_000
+    got = rips_persistence(torch.from_numpy(p).cuda(), 2.701, max_dim=1)
+    assert _same_rows(got[0].cpu(), ref["h0"])
+    assert _same_rows(got[1].cpu(), ref["h1"])
+
+
+def test_dense_h2_with_million_tetrahedron_rows_matches_oracle():
+    """H2 of a d = 50 cloud with millions of tetrahedron rows (the serving
+    stream's dense H2 requests): H2 working columns become global bitmaps
+    with a summary. H0-H2 against the oracle (H2 as a multiset)."""
+    import oracle
+    from flashph_b200 import rips_persistence
+    p = np.random.default_rng(4).standard_normal((240, 50)).astype(np.float32)
+    dd = np.sqrt(((p[:, None, :].astype(np.float64) - p[None]) ** 2).sum(-1))
+    t = float(np.quantile(dd[np.triu_indices(240, 1)], 0.30))
+    ref = oracle.run(p, t, 2, fused=True)
+    assert ref["Q"] > 1_000_000
+    got = rips_persistence(torch.from_numpy(p).cuda(), t, max_dim=2)
+    assert _same_rows(got[0].cpu(), ref["h0"])
+    assert _same_rows(got[1].cpu(), ref["h1"])
+    assert _same_rows(sorted_rows(got[2].cpu().numpy()), sorted_rows(ref["h2"]))
