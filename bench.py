@@ -5,7 +5,7 @@ max_edge_length=1.4, max_dim=2 (the reference's "20K x 10 H0-H2 ms"
 figure). Synthetic data. One step = one full rips_persistence call.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {flashph,reference}]
-                  [--workload {plain,batch,serve,precision}]
+                  [--workload {plain,batch,serve,precision,profile}] [--case NAME]
 
 The default line also carries a ``serving`` block: a seeded sample of the
 serving request stream (n log-uniform in [100, 50000], d in {4, 10, 50},
@@ -15,6 +15,8 @@ rips_persistence: throughput with every request queued at once, and p50/p99
 latency under Poisson arrivals at half the plain path's capacity.
 ``--workload batch`` runs the batching configuration (4096 clouds);
 ``--workload serve`` runs the serving stream over a rate sweep.
+``--workload profile --case NAME --steps K`` runs a fixed workload K times
+with no timing (the cases the ncu summaries under profiles/ were captured on).
 ``--workload precision`` runs the precision configuration (200000 x 50,
 max_edge_length 6.0, max_dim 1; ``--n/--d/--t/--max-dim`` override): the
 tensor-core screened edge kernel against the direct FP32 kernel, and the
@@ -381,24 +383,34 @@ def serving_summary(count, rates_rel=(0.5,), seed=7):
     return out
 
 
-def run_batching(args, rank, local):
-    """Batching configuration: diagrams/s of one batched call over every
-    cloud against plain per-call rips_persistence on a prefix of them."""
+def batching_summary(count, prefix=512, seed=11):
+    """The batching configuration: diagrams/s of rips_persistence_batch over
+    `count` clouds (two timed runs after a warm run, the faster kept) against
+    plain per-call rips_persistence on the first `prefix` of them. Completed
+    diagrams only (clouds over the reference's limits get its ValueError)."""
     import torch
     from flashph_b200 import rips_persistence
     from flashph_b200.batch import rips_persistence_batch
 
-    torch.cuda.set_device(local)
-    clouds = batching_clouds(args.clouds)
+    clouds = batching_clouds(count, seed)
     thr = _thresholds(clouds)
-    rips_persistence_batch(clouds[:8], thr[:8], 1)  # warm
+    rips_persistence_batch(clouds[:64], thr[:64], 1)  # warm
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res = rips_persistence_batch(clouds, thr, 1)
-    torch.cuda.synchronize()
-    bt = time.perf_counter() - t0
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        res = rips_persistence_batch(clouds, thr, 1)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    bt = min(times)
     ok = sum(not isinstance(r, Exception) for r in res)
-    m = min(len(clouds), max(64, args.clouds // 8))
+    m = min(len(clouds), prefix)
+    for p, t in zip(clouds[:16], thr[:16]):  # warm the per-call path
+        try:
+            rips_persistence(p, t, max_dim=1)
+        except ValueError:
+            pass
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     pok = 0
     for p, t in zip(clouds[:m], thr[:m]):
@@ -409,17 +421,76 @@ def run_batching(args, rank, local):
             pass
     torch.cuda.synchronize()
     pt = time.perf_counter() - t0
+    return {"workload": "batching: n log-uniform [64,4096], d in {3,8,32}, half N(0,1), half rotated noisy "
+                        "Clifford tori, t = 95th pct 20-NN, max_dim=1; host arrays in, device diagrams out",
+            "clouds": len(clouds), "diagrams": ok, "over_limit": len(clouds) - ok,
+            "batched_diagrams_per_s": round(ok / bt, 2), "batch_seconds": round(bt, 3),
+            "batch_runs_s": [round(x, 3) for x in times],
+            "plain_per_call": {"clouds": m, "seconds": round(pt, 3), "diagrams": pok,
+                               "diagrams_per_s": round(pok / pt, 2)},
+            "batched_over_plain": round((ok / bt) / (pok / pt), 3)}
+
+
+def run_batching(args, rank, local):
+    """Batching configuration as its own line."""
+    import torch
+    torch.cuda.set_device(local)
+    out = batching_summary(args.clouds)
     if rank == 0:
-        print(json.dumps({
-            "metric": "batched diagrams/s", "value": round(len(clouds) / bt, 2), "unit": "diagrams/s",
-            "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32",
-            "config": {"workload": "batching: n log-uniform [64,4096], d in {3,8,32}, half N(0,1), half "
-                                   "rotated noisy Clifford tori, t = 95th pct 20-NN, max_dim=1",
-                       "clouds": len(clouds), "ok": ok, "capped": len(clouds) - ok},
-            "batch_seconds": round(bt, 3),
-            "plain_per_call": {"clouds": m, "seconds": round(pt, 3), "ok": pok,
-                               "diagrams_per_s": round(m / pt, 2)},
-            "batched_over_plain": round((len(clouds) / bt) / (m / pt), 3)}), flush=True)
+        print(json.dumps({"metric": "batched diagrams/s", "value": out["batched_diagrams_per_s"],
+                          "unit": "diagrams/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+                          "dtype": "f32", "config": {"workload": out["workload"], "clouds": out["clouds"]},
+                          "batching": out}), flush=True)
+
+
+def _profile_case(case):
+    """Workloads the committed ncu summaries were captured on: (points, t,
+    max_dim) for a single call, or a callable."""
+    rng = np.random.default_rng
+    if case == "bench20k":  # the headline workload
+        return make_points(), THRESH, MAX_DIM
+    if case == "dense1898":  # a dense cloud of the batching configuration's size: 9.8M triangle rows
+        return rng(2).standard_normal((1898, 8)).astype(np.float32), 2.701, 1
+    if case == "dense_h2_382":  # a dense H2 request of the serving stream (6.1M tetrahedra)
+        return rng(4).standard_normal((382, 50)).astype(np.float32), 9.432, 2
+    if case == "reject40k":  # a serving request over the triangle limit (2.26e9 triangles)
+        return rng(3).standard_normal((40061, 50)).astype(np.float32), 7.946, 1
+    if case == "precision200k":  # the precision configuration
+        return rng(SEED).standard_normal((200000, 50)).astype(np.float32), 6.0, 1
+    raise ValueError(case)
+
+
+def run_profile(args, rank, local):
+    """A fixed workload run --steps times, for ncu captures (no timing)."""
+    import torch
+    torch.cuda.set_device(local)
+    case = args.case
+    if case == "knn20k":
+        from flashph_b200 import enclosing_radius
+        from flashph_b200.threshold import knn_kth_distance
+        x = torch.from_numpy(make_points()).cuda()
+        for _ in range(args.steps):
+            knn_kth_distance(x, 20)
+            knn_kth_distance(x, 100)
+            enclosing_radius(x)
+    elif case == "batch256":
+        from flashph_b200.batch import rips_persistence_batch
+        clouds = batching_clouds(256)
+        thr = _thresholds(clouds)
+        xs = [torch.from_numpy(c).cuda() for c in clouds]
+        for _ in range(args.steps):
+            rips_persistence_batch(xs, thr, 1)
+    else:
+        from flashph_b200 import rips_persistence
+        pts, t, md = _profile_case(case)
+        x = torch.from_numpy(pts).cuda()
+        for _ in range(args.steps):
+            try:
+                rips_persistence(x, t, max_dim=md)
+            except ValueError:
+                pass
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": case, "steps": args.steps}), flush=True)
 
 
 def run_serving(args, rank, local):
@@ -679,9 +750,9 @@ def kernel_breakdown(pts, t, max_dim, flush, reps=3):
 
 # DRAM traffic per launch from ncu captures of this workload (profiles/*.md)
 NCU_TRAFFIC = {
-    "k_tc_edges": {"bytes": 2.29e6 + 0.02e6, "source": "profiles/k_tc_edges_20k_d10.md"},
-    "k_reduce": {"bytes": 0.83e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
-    "k_cluster_sort": {"bytes": 0.391e6, "source": "profiles/k_cluster_sort_20k_d10.md"},
+    "k_tc_edges": {"bytes": 2.290e6 + 0.028e6, "source": "profiles/k_tc_edges_20k_d10.md"},
+    "k_reduce": {"bytes": 0.847e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
+    "k_cluster_sort": {"bytes": 0.389e6, "source": "profiles/k_cluster_sort_20k_d10.md"},
 }
 
 
@@ -707,8 +778,8 @@ def rooflines(stages, edge_ms, n, d, E, T, pk, src):
                        "achieved": round(gbs, 2), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 5),
                        "traffic": NCU_TRAFFIC["k_cluster_sort"]["bytes"],
                        "traffic_source": NCU_TRAFFIC["k_cluster_sort"]["source"],
-                       "traffic_note": "captured on the (key, value) form of the same sort: the same 12 bytes "
-                                       "per edge are read once",
+                       "traffic_note": "the fused filtration sort's launch: the 12 bytes per edge are read "
+                                       "once, the passes stay in distributed shared memory",
                        "algorithmic_bytes_per_launch": byts,
                        "avg_launch_ms": round(stages["sort"], 5),
                        "per_unit": "12 bytes (i, j, dist^2) read and written per edge",
@@ -792,8 +863,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--no-batching", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=96)
-    ap.add_argument("--workload", choices=("plain", "batch", "serve", "precision"), default="plain")
+    ap.add_argument("--workload", choices=("plain", "batch", "serve", "precision", "profile"), default="plain")
+    ap.add_argument("--case", default="bench20k", help="profile workload: bench20k, dense1898, dense_h2_382, "
+                                                        "reject40k, precision200k, knn20k, batch256")
     ap.add_argument("--clouds", type=int, default=4096)
     ap.add_argument("--n", type=int, default=None, help="precision workload: points")
     ap.add_argument("--d", type=int, default=None, help="precision workload: dimension")
@@ -814,6 +888,9 @@ def main():
         return
     if args.workload == "precision":
         run_precision(args, rank, local)
+        return
+    if args.workload == "profile":
+        run_profile(args, rank, local)
         return
 
     import torch
@@ -925,6 +1002,8 @@ def main():
             line["serving"] = serving_summary(args.serving_requests, rates_rel=(0.5,))
         if not args.no_precision and world == 1:
             line["precision"] = precision_block(dev)
+        if not args.no_batching and world == 1:
+            line["batching"] = batching_summary(args.clouds)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -48,22 +48,34 @@ struct GatherItem {
   int64_t count;    // floats
 };
 
-// every cloud's points into the union buffer: one block per cloud
-__global__ void k_gather_points(const GatherItem* __restrict__ items, int nclouds, float* __restrict__ dst) {
+// every cloud's points into the union buffer: a grid-stride walk over all
+// floats of the batch, each element's cloud found by binary search in the
+// clouds' destination offsets (items are in destination order), four
+// independent copies per thread in flight
+__global__ void k_gather_points(const GatherItem* __restrict__ items, int nclouds, i64 total,
+                                float* __restrict__ dst) {
   ph::pdl_wait();
   ph::pdl_trigger();
-  for (int c = blockIdx.x; c < nclouds; c += gridDim.x) {
-    const GatherItem it = items[c];
-    const bool vec = ((reinterpret_cast<uintptr_t>(it.src) | (uintptr_t)(it.dst_off * 4)) & 15) == 0;
-    if (vec) {
-      const i64 n4 = it.count / 4;
-      const float4* s4 = reinterpret_cast<const float4*>(it.src);
-      float4* d4 = reinterpret_cast<float4*>(dst + it.dst_off);
-      for (i64 i = threadIdx.x; i < n4; i += blockDim.x) d4[i] = s4[i];
-      for (i64 i = n4 * 4 + threadIdx.x; i < it.count; i += blockDim.x) dst[it.dst_off + i] = it.src[i];
-    } else {
-      for (i64 i = threadIdx.x; i < it.count; i += blockDim.x) dst[it.dst_off + i] = it.src[i];
+  const i64 stride = (i64)gridDim.x * blockDim.x;
+  for (i64 x0 = (i64)blockIdx.x * blockDim.x + threadIdx.x; x0 < total; x0 += 4 * stride) {
+    float v[4];
+    i64 at[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const i64 x = x0 + q * stride;
+      at[q] = x;
+      if (x >= total) continue;
+      int lo = 0, hi = nclouds - 1;  // last cloud with dst_off <= x
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].dst_off <= x) lo = mid;
+        else hi = mid - 1;
+      }
+      v[q] = items[lo].src[x - items[lo].dst_off];
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (at[q] < total) dst[at[q]] = v[q];
   }
 }
 
@@ -236,7 +248,8 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
   count_launch();
   ph::launch_pdl(k_zero_i64, dim3(1), dim3(32), 0, s, cnt, 16);
   count_launch();
-  ph::launch_pdl(k_gather_points, dim3((unsigned)std::min(K, 148 * 8)), dim3(256), 0, s, dgat, K, pts);
+  ph::launch_pdl(k_gather_points, dim3((unsigned)std::max<i64>(1, std::min<i64>((floats + 1023) / 1024, 148 * 16))),
+                 dim3(256), 0, s, dgat, K, floats, pts);
   PH_TRY(ph_batch_vertex_cloud(dsegs, K, vcloud, s));
 
   // ---- 1. edges --------------------------------------------------------------------------------

@@ -12,7 +12,14 @@ namespace {
 thread_local std::string g_last_error;
 std::atomic<unsigned long long> g_launches{0};
 thread_local bool g_dependent_launch = true;
+std::atomic<long long> g_reduce_max_steps{0};
+std::atomic<long long> g_reduce_first_pool{0};
 }  // namespace
+long long reduce_max_steps() {
+  const long long v = g_reduce_max_steps.load(std::memory_order_relaxed);
+  return v > 0 ? v : (1ll << 24);
+}
+long long reduce_first_pool_limit() { return g_reduce_first_pool.load(std::memory_order_relaxed); }
 void record_error(cudaError_t e) { g_last_error = cudaGetErrorString(e); }
 void record_message(const char* msg) { g_last_error = msg; }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -115,3 +122,8 @@ extern "C" unsigned long long ph_launch_count(void) {
 }
 
 extern "C" void ph_set_dependent_launch(int32_t enable) { ph::g_dependent_launch = enable != 0; }
+
+extern "C" void ph_set_reduce_limits(int64_t max_steps, int64_t first_pool_entries) {
+  ph::g_reduce_max_steps.store(max_steps > 0 ? max_steps : 0, std::memory_order_relaxed);
+  ph::g_reduce_first_pool.store(first_pool_entries > 0 ? first_pool_entries : 0, std::memory_order_relaxed);
+}

@@ -38,6 +38,10 @@ void record_message(const char* msg);
 
 // Counts kernel launches made by this library (reported by ph_launch_count()).
 void count_launch();
+// The reducer's step cap per column (ph_set_reduce_limits; 2^24 by default)
+// and the cap on a native call's first reduction pool (0: none).
+long long reduce_max_steps();
+long long reduce_first_pool_limit();
 
 // Raises a kernel's dynamic shared memory limit to the device's opt-in
 // maximum (minus the kernel's static shared memory). Always the same value,

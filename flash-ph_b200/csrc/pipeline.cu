@@ -10,8 +10,9 @@
 //   1b. on dense graphs, the exact triangle total (checked against the limit
 //       before the filtration order and the forest are built)
 //   2. the triangle count (and the H0 forest's status)
-//   3. the H1 reduction's status and row count, together with the
-//      tetrahedron count when H2 is asked for
+//   2b. with H2, the tetrahedron count (checked against the limit before
+//       the H1 columns are built)
+//   3. the H1 reduction's status and row count
 //   4. the H2 reduction's status and row count
 // The results stay on the device in a ph_result until copied out.
 #include <algorithm>
@@ -210,7 +211,11 @@ int readback_parts(const Part* parts, int nparts, const Slots& slots, cudaStream
 
 i64 pool_capacity(i64 nnz, i64 K) {
   const i64 mult = nnz < (i64(1) << 24) ? 8 : 3;
-  return std::min<i64>(mult * nnz + 2 * K + (i64(1) << 23), POOL_MAX);
+  i64 cap = std::min<i64>(mult * nnz + 2 * K + (i64(1) << 23), POOL_MAX);
+  // a test can make the first pool small to exercise the exhaustion retry
+  const long long lim = reduce_first_pool_limit();
+  if (lim > 0) cap = std::min<i64>(cap, lim);
+  return cap;
 }
 
 int reduce_only(Arena& A, cudaStream_t s, const i32* off, const i32* data, i64 K, i32 col_base, i64 R,
@@ -363,23 +368,18 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   // ---- 1b. dense graphs: the exact triangle total first --------------------------------------
   // On dense graphs the per-edge triangle count costs sum(deg^2), and a call
   // over the triangle limit (the reference's ValueError, with the exact total
-  // in its text) needs nothing but that total: it comes from a rank-free
-  // adjacency of the unsorted edges and a shared-bitmap pass, before the
-  // filtration order and the forest are built.
+  // in its text) needs nothing but that total: it comes from the unsorted
+  // edges (an upper adjacency built by counting, no sort) and a shared-bitmap
+  // pass, before the filtration order and the forest are built.
   const bool total_first = max_dim >= 1 && 4.0 * (double)E * (double)E / (double)n > 2e8 &&
                            n <= ph_triangles_total_max_vertices();
   i64 T_total = -1;
   if (total_first) {
-    i32* tp = A.take<i32>(n + 1);
-    i32* tidx = A.take<i32>(2 * E);
-    i32* trank = A.take<i32>(2 * E);
-    const size_t tcsr_b = ph_vertex_csr_workspace_bytes(E);
-    void* tcsr_ws = A.bytes(tcsr_b);
+    const size_t tt_b = ph_triangles_total_edges_workspace_bytes(E, n);
+    void* tt_ws = A.bytes(tt_b);
     if (A.failed) return alloc_fail();
-    int rc = ph_vertex_csr(ei, ej, E, n, tp, tidx, trank, tcsr_ws, tcsr_b, s);
-    if (rc == PH_OK)
-      rc = ph_triangles_total(tp, tidx, n, reinterpret_cast<unsigned long long*>(cnt + 5),
-                              reinterpret_cast<int*>(cnt + 6), s);
+    const int rc = ph_triangles_total_edges(ei, ej, E, n, reinterpret_cast<unsigned long long*>(cnt + 5), tt_ws,
+                                            tt_b, s);
     if (rc != PH_OK) return give_up(rc);
     const int64_t* src[1] = {cnt + 5};
     if (readback(src, 1, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
@@ -484,9 +484,33 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   if (A.failed || cudaMallocAsync((void**)&res->rows[1], sizeof(float) * 2 * std::max<i64>(E, 1), s) != cudaSuccess)
     return alloc_fail();
   if (T) {
-    int rc = ph_triangles_emit(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tri_m, tri_w, tri_fa, tri_fb, s);
-    if (rc == PH_OK)
-      rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
+    const int rc = ph_triangles_emit(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tri_m, tri_w, tri_fa, tri_fb, s);
+    if (rc != PH_OK) return give_up(rc);
+  }
+  // H2: the tetrahedron count only needs the triangles, and a call over the
+  // tetrahedron limit fails here, before the H1 columns are built and reduced
+  int64_t* tet_off = nullptr;
+  i64 Q = 0;
+  if (max_dim == 2) {
+    tet_off = A.take<int64_t>(E + 1);
+    const size_t tq_b = ph_tets_count_workspace_bytes(E);
+    void* tq_ws = A.bytes(tq_b);
+    if (A.failed) return alloc_fail();
+    int rc = ph_tets_count(tri_off, tri_w, E, adj_ptr, adj_idx, adj_rank, nullptr, tet_off, tq_ws, tq_b, s);
+    if (rc != PH_OK) return give_up(rc);
+    const int64_t* src[1] = {tet_off + E};
+    if (readback(src, 1, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    Q = H[0];
+    if (Q > max_tetrahedra) {
+      char m[200];
+      snprintf(m, sizeof m,
+               "Tetrahedra count %lld exceeds max_tetrahedra=%lld. Reduce max_edge_length or increase max_tetrahedra.",
+               (long long)Q, (long long)max_tetrahedra);
+      return give_up(fail(PH_ERR_LIMIT, m));
+    }
+  }
+  if (T) {
+    int rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
     if (rc == PH_OK) rc = ph_cof_max_face(nullptr, tri_m, tri_fa, tri_fb, 3, T, 0, mask, cmf1, s);
     if (rc != PH_OK) return give_up(rc);
   } else {
@@ -496,26 +520,12 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   // ---- 5. H1 reduction and rows (reduce_h1_gpu.py:159-223, 574-604) --------------------------
   i64 pool1 = pool_capacity(3 * T, E);
   RedOut r1{};
-  int64_t* tet_off = nullptr;
-  void* tq_ws = nullptr;
-  size_t tq_b = 0;
-  if (max_dim == 2) {
-    tet_off = A.take<int64_t>(E + 1);
-    tq_b = ph_tets_count_workspace_bytes(E);
-    tq_ws = A.bytes(tq_b);
-    if (A.failed) return alloc_fail();
-  }
   for (int attempt = 0;; ++attempt) {
     int rc = reduce_rows(A, s, off1, data1, E, 0, T, (i32)E, mask, cmf1, filt, nullptr, tri_m, pool1, st + 2,
                          res->rows[1], r1);
     if (rc != PH_OK) return give_up(rc);
-    if (max_dim == 2 && attempt == 0) {
-      // the tetrahedron count only needs the triangles: launch it before waiting
-      rc = ph_tets_count(tri_off, tri_w, E, adj_ptr, adj_idx, adj_rank, nullptr, tet_off, tq_ws, tq_b, s);
-      if (rc != PH_OK) return give_up(rc);
-    }
-    const int64_t* src[4] = {cnt + 2, r1.nrows, r1.info + 1, max_dim == 2 ? tet_off + E : r1.nrows};
-    if (readback(src, 4, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int64_t* src[3] = {cnt + 2, r1.nrows, r1.info + 1};
+    if (readback(src, 3, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_red = (int)(H[0] & 0xffffffff);
     if (st_red == PH_OK) break;
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
@@ -532,14 +542,6 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   }
 
   // ---- 6. H2 (triangle_kernel.py:402; cohomology_general.py) --------------------------------
-  const i64 Q = H[3];
-  if (Q > max_tetrahedra) {
-    char m[200];
-    snprintf(m, sizeof m,
-             "Tetrahedra count %lld exceeds max_tetrahedra=%lld. Reduce max_edge_length or increase max_tetrahedra.",
-             (long long)Q, (long long)max_tetrahedra);
-    return give_up(fail(PH_ERR_LIMIT, m));
-  }
   if (E + T + Q >= (int64_t(1) << 31) || 4 * Q >= (int64_t(1) << 31)) {
     char m[120];
     snprintf(m, sizeof m, "Tetrahedra count %lld exceeds the int32 rank range", (long long)Q);

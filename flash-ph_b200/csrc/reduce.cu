@@ -541,23 +541,42 @@ __device__ __forceinline__ void for_each_block(const DenseCol& D, i64 b0, i64 b1
   }
 }
 
-// for_each_block in batches: g(blocks, nb) with up to eight blocks at a time
-// (warp-uniform, ascending), so that their loads can be in flight together
+// Lane-parallel walk over the blocks of [b0, b1] whose summary bits are set:
+// one summary word (up to 32 blocks) per step, lane l taking the step's l-th
+// block, so a lane reads a whole block (128 bytes, eight 16-byte loads in
+// flight) and a step costs one memory round trip however many blocks it
+// covers. g(block, active) is called by every lane (warp-uniform control
+// flow); active is false on lanes without a block this step.
 template <typename G>
-__device__ __forceinline__ void for_each_block8(const DenseCol& D, i64 b0, i64 b1, G&& g) {
-  i64 buf[8];
-  int nb = 0;
-  for_each_block(D, b0, b1, [&](i64 b) {
+__device__ __forceinline__ void for_each_block_lanes(const DenseCol& D, i64 b0, i64 b1, G&& g) {
+  const int lane = threadIdx.x & 31;
+  for (i64 sw = (b0 >> 5); sw <= (b1 >> 5); ++sw) {
+    u32 m = sm_ld32(D.sum + sw);
+    if (sw == (b0 >> 5)) m &= ~0u << (b0 & 31);
+    if (sw == (b1 >> 5) && (b1 & 31) != 31) m &= (2u << (b1 & 31)) - 1u;
+    if (!m) continue;
+    const bool active = lane < __popc(m);
+    const i64 blk = active ? (sw << 5) + (i64)__fns(m, 0, lane + 1) : 0;
+    g(blk, active);
+  }
+}
+
+// the 32 words of block b, those outside [wlo, whi] as zero
+__device__ __forceinline__ void load_block(const DenseCol& D, i64 b, i64 wlo, i64 whi, u32 (&v)[32]) {
+  const uint4* p = reinterpret_cast<const uint4*>(D.bits + (b << 5));
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (q == nb) buf[q] = b;
-    if (++nb == 8) {
-      g(buf, 8);
-      nb = 0;
-    }
-    return true;
-  });
-  if (nb) g(buf, nb);
+  for (int q = 0; q < 8; ++q) {
+    const uint4 x = __ldcg(p + q);
+    v[4 * q + 0] = x.x;
+    v[4 * q + 1] = x.y;
+    v[4 * q + 2] = x.z;
+    v[4 * q + 3] = x.w;
+  }
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const i64 w = (b << 5) + k;
+    if (w < wlo || w > whi) v[k] = 0u;
+  }
 }
 
 // set bits of the bitmap (all at or after the pivot's word)
@@ -566,15 +585,12 @@ __device__ int dense_count(const DenseCol& D, i32 row_base) {
   int c = 0;
   const i64 w0 = (i64)((D.piv - row_base) >> 5);
   if (D.sum) {
-    for_each_block8(D, w0 >> 5, D.hi >> 5, [&](const i64* bs, int nb) {
-      u32 v[8];
+    for_each_block_lanes(D, w0 >> 5, D.hi >> 5, [&](i64 b, bool active) {
+      if (!active) return;
+      u32 v[32];
+      load_block(D, b, w0, D.hi, v);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const i64 w = (bs[q] << 5) + lane;
-        v[q] = (q < nb && w >= w0 && w <= D.hi) ? __ldcg(D.bits + w) : 0u;
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) c += __popc(v[q]);
+      for (int k = 0; k < 32; ++k) c += __popc(v[k]);
     });
     return __reduce_add_sync(FULL, c);
   }
@@ -661,32 +677,32 @@ __device__ void dense_to_list(const DenseCol& D, i32 row_base, i32* out) {
   int pos = 0;
   const i64 wp = (i64)((D.piv - row_base) >> 5);
   if (D.sum) {
-    for_each_block8(D, wp >> 5, D.hi >> 5, [&](const i64* bs, int nb) {
-      u32 v[8];
+    for_each_block_lanes(D, wp >> 5, D.hi >> 5, [&](i64 b, bool active) {
+      u32 v[32];
+      int c = 0;
+      if (active) {
+        load_block(D, b, wp, D.hi, v);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const i64 w = (bs[q] << 5) + lane;
-        v[q] = (q < nb && w >= wp && w <= D.hi) ? __ldcg(D.bits + w) : 0u;
+        for (int k = 0; k < 32; ++k) c += __popc(v[k]);
       }
+      int incl = c;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        if (q >= nb) break;
-        const i64 w = (bs[q] << 5) + lane;
-        u32 x = v[q];
-        const int c = __popc(x);
-        int incl = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(FULL, incl, o);
-          if (lane >= o) incl += t;
-        }
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+      }
+      if (active) {  // the lane's block is the lane-th of the step in ascending order
         int at = pos + incl - c;
-        while (x) {
-          out[at++] = (i32)((w << 5) + (__ffs(x) - 1)) + row_base;
-          x &= x - 1;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          u32 x = v[k];
+          while (x) {
+            out[at++] = (i32)((((b << 5) + k) << 5) + (__ffs(x) - 1)) + row_base;
+            x &= x - 1;
+          }
         }
-        pos += __shfl_sync(FULL, incl, 31);
       }
+      pos += __shfl_sync(FULL, incl, 31);
     });
     __syncwarp();
     return;
@@ -721,9 +737,11 @@ __device__ void dense_sum_zero(DenseCol& D, i64 b0, i64 b1) {
 __device__ void dense_clear(DenseCol& D, i64 lo, i64 hi) {
   const int lane = threadIdx.x & 31;
   if (D.sum && hi >= lo) {  // only the blocks that may hold set bits
-    for_each_block(D, lo >> 5, hi >> 5, [&](i64 b) {
-      __stcg(D.bits + (b << 5) + lane, 0u);
-      return true;
+    for_each_block_lanes(D, lo >> 5, hi >> 5, [&](i64 b, bool active) {
+      if (!active) return;
+      uint4* p = reinterpret_cast<uint4*>(D.bits + (b << 5));
+#pragma unroll
+      for (int q = 0; q < 8; ++q) __stcg(p + q, make_uint4(0u, 0u, 0u, 0u));
     });
     __syncwarp();
     dense_sum_zero(D, lo >> 5, hi >> 5);
@@ -1059,8 +1077,9 @@ int reduce_blocks(i64 K) {
 // A dense working column's bitmap starts at the word of its first pivot and
 // must hold every row its entries can reach: `span` rows (all R rows for a
 // single cloud; in a batch, the largest row range of one cloud, since a
-// column only ever meets rows of its own cloud), plus a word of alignment.
-i64 window_words(i64 span) { return (span + 31) / 32 + 2; }
+// column only ever meets rows of its own cloud), plus a word of alignment,
+// rounded up to whole 32-word blocks (slots and blocks 128-byte aligned).
+i64 window_words(i64 span) { return ((span + 31) / 32 + 2 + 31) / 32 * 32; }
 
 // words of the shared-memory bitmap each warp uses for every working column,
 // 0 when the window does not fit one working buffer
@@ -1124,7 +1143,8 @@ extern "C" int ph_reduce(const int32_t* cof_off, const int32_t* cof_data, int64_
   const int chunk = (int)std::max<i64>(64, std::min<i64>(2048, pool_cap / (4 * (i64)blocks * RD_WARPS)));
   ph::count_launch();
   ph::launch_pdl(k_reduce, dim3(blocks), dim3(RD_NT), RD_SMEM, s, row_base, K, col_state, rec, owner, pool, pool_cap, chunk, ctl, d_status,
-                                          1 << 24, dense, dw, sm_dense_words(span));
+                                          (int)std::min<long long>(ph::reduce_max_steps(), INT_MAX), dense, dw,
+                                          sm_dense_words(span));
   ph::count_launch();
   ph::launch_pdl(k_finish_cols, dim3(grid_for(K)), dim3(256), 0, s, K, col_state, col_piv, ctl, d_info);
   if (R > 0) {

@@ -106,6 +106,10 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
 // bitmap, each warp takes a neighbour b > a and tests its neighbours w > b
 // against the bitmap. No ranks are needed, since every triangle has exactly
 // one largest edge; the result equals the sum of the per-edge triangle counts.
+// UPPER: the rows hold only the larger neighbours, in any order (the upper
+// adjacency of k_upper_fill), so no row is searched; otherwise the rows are
+// the full adjacency sorted by neighbour.
+template <bool UPPER>
 __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ aptr, const i32* __restrict__ aidx,
                                                     i64 n, int* __restrict__ next,
                                                     unsigned long long* __restrict__ total) {
@@ -130,12 +134,12 @@ __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ apt
       atomicOr(&nbits[v >> 5], 1u << (v & 31));
     }
     __syncthreads();
-    // neighbours b > a of a (rows sorted by neighbour index)
-    const int first = lower_bound_i32(aidx, s, e, (i32)a + 1);
+    // neighbours b > a of a (sorted rows: from the first one above a)
+    const int first = UPPER ? s : lower_bound_i32(aidx, s, e, (i32)a + 1);
     for (int p = first + warp; p < e; p += SX_NT / 32) {
       const i32 b = aidx[p];
       const int sb = aptr[b], eb = aptr[b + 1];
-      for (int q = lower_bound_i32(aidx, sb, eb, b + 1) + lane; q < eb; q += 32) {
+      for (int q = (UPPER ? sb : lower_bound_i32(aidx, sb, eb, b + 1)) + lane; q < eb; q += 32) {
         const i32 w = aidx[q];
         cnt += (nbits[w >> 5] >> (w & 31)) & 1u;
       }
@@ -148,6 +152,24 @@ __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ apt
   }
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
   if (lane == 0 && cnt) atomicAdd(total, cnt);
+}
+
+// upper adjacency of unsorted edges i < j: row i lists every j, in any order
+__global__ void k_upper_deg(const i32* __restrict__ ei, i64 E, i32* __restrict__ deg) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x)
+    atomicAdd(&deg[ei[e]], 1);
+}
+
+__global__ void k_upper_fill(const i32* __restrict__ ei, const i32* __restrict__ ej, i64 E,
+                             const i32* __restrict__ uptr, i32* __restrict__ cursor, i32* __restrict__ uidx) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (i64)gridDim.x * blockDim.x) {
+    const i32 i = ei[e];
+    uidx[uptr[i] + atomicAdd(&cursor[i], 1)] = ej[e];
+  }
 }
 
 // Tetrahedra with largest edge m: pairs (i < k) of m's triangles whose third
@@ -331,15 +353,63 @@ extern "C" int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx
     return PH_OK;
   }
   const size_t smem = (size_t)((n + 31) / 32) * 4;
-  if (smem > 48 * 1024 && ph::allow_dynamic_smem((const void*)k_tri_total) != cudaSuccess) {
+  if (smem > 48 * 1024 && ph::allow_dynamic_smem((const void*)k_tri_total<false>) != cudaSuccess) {
     PH_CHECK_LAUNCH();
     return PH_ERR_CUDA;
   }
   const int sms = ph::device_sms();
-  const int occ = ph::occupancy((const void*)k_tri_total, SX_NT, smem);
+  const int occ = ph::occupancy((const void*)k_tri_total<false>, SX_NT, smem);
   const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
   ph::count_launch();
-  ph::launch_pdl(k_tri_total, dim3(grid), dim3(SX_NT), smem, s, adj_ptr, adj_idx, n, d_next, d_total);
+  ph::launch_pdl(k_tri_total<false>, dim3(grid), dim3(SX_NT), smem, s, adj_ptr, adj_idx, n, d_next, d_total);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" size_t ph_triangles_total_edges_workspace_bytes(int64_t E, int64_t n) {
+  return Carve::need(sizeof(i32) * (size_t)(n + 1)) * 3 + Carve::need(sizeof(i32) * (size_t)std::max<i64>(E, 1)) +
+         Carve::need(scan_workspace_bytes(n)) + Carve::need(sizeof(int));
+}
+
+extern "C" int ph_triangles_total_edges(const int32_t* edge_i, const int32_t* edge_j, int64_t E, int64_t n,
+                                        unsigned long long* d_total, void* workspace, size_t workspace_bytes,
+                                        void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (E < 0 || n < 0 || !d_total || E >= (int64_t(1) << 31)) return PH_ERR_ARG;
+  if (n > ph_triangles_total_max_vertices()) {
+    record_message("ph_triangles_total_edges: n exceeds the shared-memory bitmap (1638400 vertices)");
+    return PH_ERR_ARG;
+  }
+  Carve c(workspace, workspace_bytes);
+  i32* deg = c.take<i32>(n + 1);
+  i32* uptr = c.take<i32>(n + 1);
+  i32* cursor = c.take<i32>(n + 1);
+  i32* uidx = c.take<i32>(std::max<i64>(E, 1));
+  void* sws = c.take<char>((i64)scan_workspace_bytes(n));
+  int* next = c.take<int>(1);
+  if (!deg || !uptr || !cursor || !uidx || !sws || !next) return PH_ERR_ARG;
+  ph::zero_async(d_total, sizeof(unsigned long long), s, next, sizeof(int));
+  if (n < 3 || E < 3) {
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  ph::zero_async(deg, sizeof(i32) * (n + 1), s, cursor, sizeof(i32) * (n + 1));
+  ph::count_launch();
+  ph::launch_pdl(k_upper_deg, dim3(grid_for(E)), dim3(256), 0, s, edge_i, E, deg);
+  PH_TRY(scan_exclusive_i32_i32(deg, uptr, n, sws, scan_workspace_bytes(n), s));
+  ph::count_launch();
+  ph::launch_pdl(k_upper_fill, dim3(grid_for(E)), dim3(256), 0, s, edge_i, edge_j, E, (const i32*)uptr, cursor, uidx);
+  const size_t smem = (size_t)((n + 31) / 32) * 4;
+  if (smem > 48 * 1024 && ph::allow_dynamic_smem((const void*)k_tri_total<true>) != cudaSuccess) {
+    PH_CHECK_LAUNCH();
+    return PH_ERR_CUDA;
+  }
+  const int sms = ph::device_sms();
+  const int occ = ph::occupancy((const void*)k_tri_total<true>, SX_NT, smem);
+  const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
+  ph::count_launch();
+  ph::launch_pdl(k_tri_total<true>, dim3(grid), dim3(SX_NT), smem, s, (const i32*)uptr, (const i32*)uidx, n, next,
+                 d_total);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -102,8 +102,11 @@ __global__ void __launch_bounds__(KN_NT) k_knn_top(const float* __restrict__ pts
     const i64 g = cv.qblk * KN_NT + t;
     q[kk * KN_NT + t] = g < n ? pts[g * d + kk] : 0.0f;
   }
+  // the sorted list lives in local memory (indexed by a variable); its largest
+  // entry, the only one every candidate is compared with, stays in a register
   float best[KN_MAXK];
   for (int z = 0; z < KN_MAXK; ++z) best[z] = __int_as_float(0x7f800000);
+  float tau = __int_as_float(0x7f800000);
   for (i64 j0 = 0; j0 < n; j0 += KN_TP) {
     __syncthreads();
     const int tp = (int)((n - j0) < (i64)KN_TP ? (n - j0) : (i64)KN_TP);
@@ -117,17 +120,18 @@ __global__ void __launch_bounds__(KN_NT) k_knn_top(const float* __restrict__ pts
         const float df = __fsub_rn(q[kk * KN_NT + threadIdx.x], tile[jj * d + kk]);
         acc = __fmaf_rn(df, df, acc);
       }
-      if (j != qi && acc < best[k - 1]) {
+      if (acc < tau && j != qi) {
         int z = k - 1;
         while (z > 0 && best[z - 1] > acc) {
           best[z] = best[z - 1];
           --z;
         }
         best[z] = acc;
+        tau = best[k - 1];
       }
     }
   }
-  if (qi < n) out[cv.out_off + qi] = k >= 1 ? __fsqrt_rn(best[k - 1]) : 0.0f;
+  if (qi < n) out[cv.out_off + qi] = k >= 1 ? __fsqrt_rn(tau) : 0.0f;
 }
 
 // ---- chunked distance tile (select and enclosing) ------------------------------------

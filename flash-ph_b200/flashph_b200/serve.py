@@ -1,23 +1,33 @@
-"""Serving form: a continuous-batching request loop on one GPU.
+"""Serving form: continuous batching of rips_persistence requests on one GPU.
 
 ``PersistenceServer.submit(points, max_edge_length, max_dim)`` returns a
-future. Worker slots (one CUDA stream each) take work from the queue: a
-request of at least ``solo_min_points`` points runs alone through the native
-pipeline (``ph_rips_persistence``, one library call that waits on the host
-four times at most); the small requests at the head of the queue that fit
-the admission limits run together as one batch through the batching
-pipeline (``batch.rips_persistence_batch``), which spreads a call's fixed
-cost over them; a small request with no company runs alone too. Defaults:
-one slot and every request native (``solo_min_points=0``). On the serving
-stream neither several slots (streams at once) nor batching the small
-requests measured faster than one native call at a time, which already keeps
-the GPU busy; both remain available as parameters. Admission is by memory, estimated
-from the request sizes (points, candidate pairs); the pipelines' own
-counting passes enforce the reference's per-call triangle and tetrahedron
-caps per request.
+future. Worker slots (one CUDA stream each, ``slots`` of them) take work from
+the queue as soon as they are free, so requests that arrive while others are
+on the GPU join the next batch, whose requests run together as one union on
+the device:
 
-Every result equals what ``rips_persistence`` returns for that request
-alone, bit for bit: requests never interact inside a batch.
+* a request of at least ``solo_min_points`` points runs alone through the
+  native single-cloud call (``ph_rips_persistence``: its stages are sized to
+  the one cloud, and a dense request over the triangle limit fails after its
+  exact triangle total, before the filtration order is built);
+* the smaller requests waiting in the queue are admitted together, in arrival
+  order, up to the admission limits (points and candidate pairs of the batch,
+  the request count), and run as one disjoint union through the native batch
+  call (``ph_rips_persistence_batch``): one library call with four host waits
+  for the whole batch. Its first stages are a counting pass: the exact
+  per-request edge, triangle and tetrahedron counts decide, on the device
+  side of the call, which requests exceed the reference's limits and whether
+  the batch fits its simplex budget (a batch over the budget is split by
+  those exact counts before any simplex is stored, which bounds the device
+  memory of a batch).
+
+Device memory stays resident between batches: every slot allocates from the
+device's stream-ordered pool, which keeps its memory for the process (the
+library sets the release threshold), and each slot reuses its own stream.
+
+Every result equals what ``rips_persistence`` returns for that request alone,
+bit for bit: requests never interact inside a batch. A request over one of the
+reference's limits resolves its future with the reference's ValueError.
 """
 from __future__ import annotations
 
@@ -52,31 +62,36 @@ class PersistenceServer:
 
     Parameters
     ----------
-    slots : concurrent batches in flight (each on its own stream; default 1).
-    max_batch_points : admission limit on the points of one batch.
-    max_batch_pairs : admission limit on candidate point pairs of one batch.
-    max_batch_requests : admission limit on requests per batch.
-    solo_min_points : requests this large run alone (native pipeline, the
-        default for all); smaller ones are batched when more than one waits.
+    slots : batches in flight at once, each on its own stream (default 1:
+        on the serving stream, two or three slots measured slower, 109 and
+        93 against 166 diagrams/s, since the heavy requests' persistent
+        kernels each fill the GPU and contend when they run together).
+    solo_min_points : requests this large run alone through the single-cloud
+        call (default 1024, the best of 1024 and 4096 measured); smaller ones
+        are batched.
+    max_batch_points, max_batch_pairs, max_batch_requests : admission limits
+        of one batch (points, candidate point pairs, requests).
+    max_triangles, max_tetrahedra : the reference's per-request limits.
     """
 
-    def __init__(self, device=None, slots: int = 1, max_batch_points: int = 1 << 17,
-                 max_batch_pairs: int = 1 << 32, max_batch_requests: int = 1024,
-                 max_triangles: int = 10_000_000, max_tetrahedra: int = 10_000_000,
-                 solo_min_points: int = 0):
+    def __init__(self, device=None, slots: int = 1, solo_min_points: int = 1024,
+                 max_batch_points: int = 1 << 18, max_batch_pairs: int = 1 << 32,
+                 max_batch_requests: int = 1024, max_triangles: int = 10_000_000,
+                 max_tetrahedra: int = 10_000_000):
         if not torch.cuda.is_available():
             raise RuntimeError("flashph_b200 computes on a CUDA device; none is available")
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.solo_min_points = solo_min_points
         self.max_batch_points = max_batch_points
         self.max_batch_pairs = max_batch_pairs
         self.max_batch_requests = max_batch_requests
         self.max_triangles = max_triangles
         self.max_tetrahedra = max_tetrahedra
-        self.solo_min_points = solo_min_points
         self._queue: collections.deque[_Request] = collections.deque()
         self._cv = threading.Condition()
         self._closed = False
         self.batches = 0
+        self.batch_sizes: list[int] = []
         self._workers = [threading.Thread(target=self._worker, args=(i,), daemon=True, name=f"ph-slot-{i}")
                          for i in range(slots)]
         for w in self._workers:
@@ -106,19 +121,25 @@ class PersistenceServer:
         self.close()
 
     def _admit(self) -> list[_Request]:
-        if self._queue[0].n >= self.solo_min_points:
+        """The next unit of work: the oldest request alone when it is large,
+        else the waiting small requests in arrival order up to the limits
+        (large ones stay queued for the next free slot)."""
+        head = self._queue[0]
+        if head.n >= self.solo_min_points:
             return [self._queue.popleft()]
-        batch, pts, pairs = [], 0, 0
+        batch, keep, pts, pairs = [], collections.deque(), 0, 0
         while self._queue and len(batch) < self.max_batch_requests:
-            r = self._queue[0]
-            n = r.n
-            if n >= self.solo_min_points:
+            r = self._queue.popleft()
+            if r.n >= self.solo_min_points:
+                keep.append(r)
+                continue
+            if batch and (pts + r.n > self.max_batch_points or pairs + r.n * r.n // 2 > self.max_batch_pairs):
+                self._queue.appendleft(r)
                 break
-            if batch and (pts + n > self.max_batch_points or pairs + n * n // 2 > self.max_batch_pairs):
-                break
-            batch.append(self._queue.popleft())
-            pts += n
-            pairs += n * n // 2
+            batch.append(r)
+            pts += r.n
+            pairs += r.n * r.n // 2
+        self._queue.extendleft(reversed(keep))
         return batch
 
     def _worker(self, index: int):
@@ -137,7 +158,7 @@ class PersistenceServer:
                 batch = self._admit()
             try:
                 with torch.cuda.stream(stream):
-                    if len(batch) == 1:  # a large request, or a small one with no company: one native call
+                    if len(batch) == 1 and batch[0].n >= self.solo_min_points:
                         r = batch[0]
                         try:
                             res = [rips_persistence(r.points, r.t, max_dim=r.max_dim)]
@@ -147,17 +168,26 @@ class PersistenceServer:
                         res = rips_persistence_batch([r.points for r in batch], [r.t for r in batch],
                                                      [r.max_dim for r in batch], self.max_triangles,
                                                      self.max_tetrahedra)
+                        # rips_persistence returns a CPU tensor's diagrams on the CPU
+                        res = [[d.cpu() for d in out] if not isinstance(out, Exception) and _on_cpu(r.points)
+                               else out for r, out in zip(batch, res)]
                 stream.synchronize()
-                self.batches += 1
             except Exception as ex:  # a failure of the whole batch goes to each request
                 res = [ex] * len(batch)
             now = time.perf_counter()
+            with self._cv:
+                self.batches += 1
+                self.batch_sizes.append(len(batch))
             for r, out in zip(batch, res):
                 r.done = now
                 if isinstance(out, Exception):
                     r.future.set_exception(out)
                 else:
                     r.future.set_result(out)
+
+
+def _on_cpu(points) -> bool:
+    return isinstance(points, torch.Tensor) and points.device.type != "cuda"
 
 
 def latency_percentiles(arrivals, completions, qs=(50, 99)):

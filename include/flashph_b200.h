@@ -54,6 +54,15 @@ unsigned long long ph_launch_count(void);
  * the reference (a launch policy of this library). */
 void ph_set_dependent_launch(int32_t enable);
 
+/* Test-only limits of the Z/2 reduction, process-wide: the most steps
+ * (column additions and pivot claims) one column may take before
+ * ph_reduce reports PH_ERR_ITER_LIMIT (default 2^24), and a cap on the
+ * reduction pool of the native calls' first attempt (a pool that runs out is
+ * retried 4x larger). 0 restores a default. No counterpart in the reference
+ * (whose Numba loops have no such bounds); used to exercise the failure paths
+ * without a device fault. */
+void ph_set_reduce_limits(int64_t max_steps, int64_t first_pool_entries);
+
 /* ---- filtration -------------------------------------------------------- */
 
 /* One point cloud of a batch. A batch is the disjoint union of its clouds:
@@ -203,6 +212,16 @@ int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, int64_t E,
 int64_t ph_triangles_total_max_vertices(void);
 int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx, int64_t n,
                        unsigned long long* d_total, int* d_next, void* stream);
+
+/* ph_triangles_total from the unsorted edges (i < j, any order), without the
+ * adjacency: an upper adjacency (row i lists the j of every edge (i, j)) is
+ * built by counting, then the same bitmap pass runs. The total the count pass
+ * of triangle_kernel.py:288 triangle_enumerate checks against max_triangles
+ * (triangle_kernel.py:377-381), for a call that may be over the limit, before
+ * any filtration order exists. n <= ph_triangles_total_max_vertices(). */
+size_t ph_triangles_total_edges_workspace_bytes(int64_t E, int64_t n);
+int ph_triangles_total_edges(const int32_t* edge_i, const int32_t* edge_j, int64_t E, int64_t n,
+                             unsigned long long* d_total, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Writes, for every triangle in global order, its largest edge tri_m, third
  * vertex tri_w and the ranks of its two other edges (a,w) and (b,w): the emit
