@@ -10,9 +10,10 @@
 //   1b. on dense graphs, the exact triangle total (checked against the limit
 //       before the filtration order and the forest are built)
 //   2. the triangle count (and the H0 forest's status)
-//   2b. with H2, the tetrahedron count (checked against the limit before
-//       the H1 columns are built)
-//   3. the H1 reduction's status and row count
+//   2b. with H2 on a dense complex, the tetrahedron count (checked against
+//       the limit before the H1 columns are built)
+//   3. the H1 reduction's status and row count (with the tetrahedron count
+//      when H2 is asked for and it was not read at 2b)
 //   4. the H2 reduction's status and row count
 // The results stay on the device in a ph_result until copied out.
 #include <algorithm>
@@ -487,10 +488,13 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     const int rc = ph_triangles_emit(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tri_m, tri_w, tri_fa, tri_fb, s);
     if (rc != PH_OK) return give_up(rc);
   }
-  // H2: the tetrahedron count only needs the triangles, and a call over the
-  // tetrahedron limit fails here, before the H1 columns are built and reduced
+  // H2: the tetrahedron count only needs the triangles. On a dense complex
+  // (T >= 16 E) it is read back here, so that a call over the tetrahedron
+  // limit fails before the H1 columns are built and reduced; otherwise it is
+  // launched here and read back with the H1 status (one host wait fewer)
   int64_t* tet_off = nullptr;
   i64 Q = 0;
+  const bool tets_first = max_dim == 2 && T >= 16 * E;
   if (max_dim == 2) {
     tet_off = A.take<int64_t>(E + 1);
     const size_t tq_b = ph_tets_count_workspace_bytes(E);
@@ -498,16 +502,21 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (A.failed) return alloc_fail();
     int rc = ph_tets_count(tri_off, tri_w, E, adj_ptr, adj_idx, adj_rank, nullptr, tet_off, tq_ws, tq_b, s);
     if (rc != PH_OK) return give_up(rc);
+  }
+  auto tets_limit = [&]() -> int {
+    if (Q <= max_tetrahedra) return PH_OK;
+    char m[200];
+    snprintf(m, sizeof m,
+             "Tetrahedra count %lld exceeds max_tetrahedra=%lld. Reduce max_edge_length or increase max_tetrahedra.",
+             (long long)Q, (long long)max_tetrahedra);
+    return fail(PH_ERR_LIMIT, m);
+  };
+  if (tets_first) {
     const int64_t* src[1] = {tet_off + E};
     if (readback(src, 1, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     Q = H[0];
-    if (Q > max_tetrahedra) {
-      char m[200];
-      snprintf(m, sizeof m,
-               "Tetrahedra count %lld exceeds max_tetrahedra=%lld. Reduce max_edge_length or increase max_tetrahedra.",
-               (long long)Q, (long long)max_tetrahedra);
-      return give_up(fail(PH_ERR_LIMIT, m));
-    }
+    const int rc = tets_limit();
+    if (rc != PH_OK) return give_up(rc);
   }
   if (T) {
     int rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
@@ -524,8 +533,8 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     int rc = reduce_rows(A, s, off1, data1, E, 0, T, (i32)E, mask, cmf1, filt, nullptr, tri_m, pool1, st + 2,
                          res->rows[1], r1);
     if (rc != PH_OK) return give_up(rc);
-    const int64_t* src[3] = {cnt + 2, r1.nrows, r1.info + 1};
-    if (readback(src, 3, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int64_t* src[4] = {cnt + 2, r1.nrows, r1.info + 1, max_dim == 2 ? tet_off + E : r1.nrows};
+    if (readback(src, 4, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_red = (int)(H[0] & 0xffffffff);
     if (st_red == PH_OK) break;
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
@@ -535,6 +544,11 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   }
   res->nrows[1] = H[1];
   res->stats[3] = H[2];
+  if (max_dim == 2 && !tets_first) {
+    Q = H[3];
+    const int rc = tets_limit();
+    if (rc != PH_OK) return give_up(rc);
+  }
   if (max_dim == 1) {
     A.release_to(res->scratch);
     *out = res;
