@@ -244,7 +244,8 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
     record_error(cudaGetLastError());
     return give_up(PH_ERR_CUDA);
   }
-  int* st = reinterpret_cast<int*>(cnt + 1);  // st[0] edges, [1] forest, [2] H1, [3] tetrahedra, [4] H2
+  // st[0] edges, [1] forest, [2] H1, [3] tetrahedra, [4] H2, [5] cofacet rows
+  int* st = reinterpret_cast<int*>(cnt + 1);
   count_launch();
   ph::launch_pdl(k_zero_i64, dim3(1), dim3(32), 0, s, cnt, 16);
   count_launch();
@@ -353,6 +354,7 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
   void* tc_ws = A.bytes(tc_b);
   if (A.failed) return alloc_fail();
   PH_TRY(ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s));
+  PH_TRY(ph_max_count(tcof_off, E, cnt + 8, s));  // the longest cofacet row (before any clearing: a bound)
   count_launch();
   ph::launch_pdl(k_seg_diff, dim3(grid_for(K)), dim3(256), 0, s, (const int64_t*)tri_off, (const int64_t*)e_off, K,
                  per);
@@ -403,6 +405,7 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
     ph::launch_pdl(k_edge_flags, dim3(grid_for(E)), dim3(256), 0, s, (const i32*)si, E, (const i32*)vcloud,
                    (const uint8_t*)cflag, 0, (const uint8_t*)nullptr, eflag);
     PH_TRY(mask_offsets(A, s, tri_off, E, eflag));
+    PH_TRY(mask_offsets(A, s, tcof_off, E, eflag));  // their cofacet rows go too
   }
   i32* tri_m = A.take<i32>(T);
   i32* tri_w = A.take<i32>(T);
@@ -419,9 +422,19 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
   void* r1_ws = A.bytes(r1_b);
   if (A.failed || cudaMallocAsync((void**)&res->rows[1], sizeof(float) * 2 * std::max<i64>(E, 1), s) != cudaSuccess)
     return alloc_fail();
+  const i64 max_row = hcnt[8];
   if (T) {
     int rc = ph_triangles_emit(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tri_m, tri_w, tri_fa, tri_fb, s);
-    if (rc == PH_OK) rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
+    // rows scattered and sorted in shared memory when every row fits, else the radix form
+    if (rc == PH_OK && max_row <= ph_cofacet_rows3_max_row()) {
+      const size_t r3_b = ph_cofacet_rows3_workspace_bytes(E);
+      void* r3_ws = A.bytes(r3_b);
+      if (A.failed) return alloc_fail();
+      rc = ph_cofacet_rows3(tri_m, tri_fa, tri_fb, T, E, (i32)E, tcof_off, (int32_t)max_row, off1, data1, st + 5,
+                            r3_ws, r3_b, s);
+    } else if (rc == PH_OK) {
+      rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
+    }
     if (rc == PH_OK) rc = ph_cof_max_face(nullptr, tri_m, tri_fa, tri_fb, 3, T, 0, mask, cmf1, s);
     if (rc != PH_OK) return give_up(rc);
   } else {
@@ -472,6 +485,7 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
                      {per, hper, any_h2 ? sizeof(int64_t) * K : 0}};
     if (readback_parts(parts, 3, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_red = (int)(hcnt[2] & 0xffffffff);
+    if ((int)(hcnt[3] >> 32) != 0) return give_up(fail((int)(hcnt[3] >> 32), "ph_cofacet_rows3 failed"));
     if (st_red == PH_OK) break;
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
       return give_up(fail(st_red, "ph_reduce (H1) failed"));

@@ -448,11 +448,13 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   if (A.failed) return alloc_fail();
   {
     int rc = ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s);
+    if (rc == PH_OK) rc = ph_max_count(tcof_off, E, cnt + 7, s);  // the longest cofacet row
     if (rc != PH_OK) return give_up(rc);
-    const int64_t* src[2] = {tri_off + E, cnt + 1};
-    if (readback(src, 2, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
+    const int64_t* src[3] = {tri_off + E, cnt + 1, cnt + 7};
+    if (readback(src, 3, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
   }
   const i64 T = H[0];
+  const i64 max_row = H[2];
   if ((int)(H[1] >> 32) != 0) return give_up(fail((int)(H[1] >> 32), "ph_boruvka_mst failed"));
   if (T_total >= 0 && T != T_total) {
     char m[160];
@@ -519,7 +521,18 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (rc != PH_OK) return give_up(rc);
   }
   if (T) {
-    int rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
+    // the rows' lengths are the cofacet counts: scattered and sorted per row
+    // when every row fits the shared-memory sort, else the radix form
+    int rc;
+    if (max_row <= ph_cofacet_rows3_max_row()) {
+      const size_t r3_b = ph_cofacet_rows3_workspace_bytes(E);
+      void* r3_ws = A.bytes(r3_b);
+      if (A.failed) return alloc_fail();
+      rc = ph_cofacet_rows3(tri_m, tri_fa, tri_fb, T, E, (i32)E, tcof_off, (int32_t)max_row, off1, data1, st + 3,
+                            r3_ws, r3_b, s);
+    } else {
+      rc = ph_cofacet_csr(nullptr, tri_m, tri_fa, tri_fb, 3, T, E, (i32)E, off1, data1, cc_ws, cc_b, s);
+    }
     if (rc == PH_OK) rc = ph_cof_max_face(nullptr, tri_m, tri_fa, tri_fb, 3, T, 0, mask, cmf1, s);
     if (rc != PH_OK) return give_up(rc);
   } else {
@@ -536,6 +549,8 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     const int64_t* src[4] = {cnt + 2, r1.nrows, r1.info + 1, max_dim == 2 ? tet_off + E : r1.nrows};
     if (readback(src, 4, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
     const int st_red = (int)(H[0] & 0xffffffff);
+    // the word beside it: the cofacet rows' status (the tetrahedra's only later)
+    if ((int)(H[0] >> 32) != 0) return give_up(fail((int)(H[0] >> 32), "ph_cofacet_rows3 failed"));
     if (st_red == PH_OK) break;
     if (st_red != PH_ERR_POOL || attempt >= 3 || pool1 >= POOL_MAX)
       return give_up(fail(st_red, "ph_reduce (H1) failed"));

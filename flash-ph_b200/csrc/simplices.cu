@@ -18,6 +18,7 @@
 // adjacency row and binary-search the longer one; ballots keep the output in
 // order.
 #include <algorithm>
+#include <climits>
 
 #include "prim.cuh"
 
@@ -25,6 +26,13 @@ namespace ph {
 namespace {
 
 constexpr int SX_NT = 256;
+constexpr int SX_WARPS = SX_NT / 32;
+// Entries of an adjacency row a warp copies into its shared memory before
+// searching it many times (dense graphs: rows of a few hundred entries,
+// searched by every candidate of the other row): a search then costs shared-
+// memory latency per step instead of a dependent global load. 8 warps x 576
+// entries x (index, rank) = 36 KB a block.
+constexpr int SX_STAGE = 576;
 constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ int lower_bound_i32(const i32* __restrict__ a, int lo, int hi, i32 x) {
@@ -48,11 +56,14 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
                                                     i32* __restrict__ tfb) {
   ph::pdl_wait();
   ph::pdl_trigger();
-  const int lane = threadIdx.x & 31;
+  __shared__ i32 st_idx[SX_WARPS][SX_STAGE];
+  __shared__ i32 st_rank[SX_WARPS][SX_STAGE];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
   const u32 lt = lanemask_lt();
   for (i64 m = warp; m < E; m += nwarps) {
+    __syncwarp();  // the previous edge's searches of the staged row are done
     const i32 a = ei[m], b = ej[m];
     int sa = aptr[a], ea = aptr[a + 1], sb = aptr[b], eb = aptr[b + 1];
     // walk the shorter row, search the longer
@@ -66,6 +77,16 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
     // triangles of some clouds after the count) is skipped
     const i64 oend = EMIT ? tri_off[m + 1] : 0;
     if (EMIT && oend <= out) continue;
+    // a long row searched by more than one round of lanes is staged first
+    const int nl = l1 - l0;
+    const bool staged = nl > 32 && nl <= SX_STAGE && s1 - s0 > 32;
+    if (staged) {
+      for (int k = lane; k < nl; k += 32) {
+        st_idx[wl][k] = aidx[l0 + k];
+        st_rank[wl][k] = arank[l0 + k];
+      }
+      __syncwarp();
+    }
     for (int base = s0; base < s1; base += 32) {
       const int p = base + lane;
       bool common = false, valid = false;
@@ -73,11 +94,20 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
       if (p < s1) {
         w = aidx[p];
         rs = arank[p];
-        const int q = lower_bound_i32(aidx, l0, l1, w);
-        if (q < l1 && aidx[q] == w) {
-          common = true;
-          rl = arank[q];
-          valid = rs < (i32)m && rl < (i32)m;
+        if (staged) {
+          const int q = lower_bound_i32(st_idx[wl], 0, nl, w);
+          if (q < nl && st_idx[wl][q] == w) {
+            common = true;
+            rl = st_rank[wl][q];
+            valid = rs < (i32)m && rl < (i32)m;
+          }
+        } else {
+          const int q = lower_bound_i32(aidx, l0, l1, w);
+          if (q < l1 && aidx[q] == w) {
+            common = true;
+            rl = arank[q];
+            valid = rs < (i32)m && rl < (i32)m;
+          }
         }
       }
       const u32 cb = __ballot_sync(FULL, common);
@@ -184,7 +214,9 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
                                                i32* __restrict__ qm, i32* __restrict__ qf, int* status) {
   ph::pdl_wait();
   ph::pdl_trigger();
-  const int lane = threadIdx.x & 31;
+  __shared__ i32 st_idx[SX_WARPS][SX_STAGE];
+  __shared__ i32 st_rank[SX_WARPS][SX_STAGE];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const i64 warp = ((i64)blockIdx.x * SX_NT + threadIdx.x) >> 5;
   const i64 nwarps = ((i64)gridDim.x * SX_NT) >> 5;
   const u32 lt = lanemask_lt();
@@ -197,16 +229,35 @@ __global__ void __launch_bounds__(SX_NT) k_tets(const i32* __restrict__ ei, cons
     for (int i = 0; i + 1 < nw; ++i) {
       const i32 p = tw[t0 + i];
       const int sp = aptr[p], ep = aptr[p + 1];
+      // N(p) searched by more than one round of lanes: staged first
+      const int np = ep - sp;
+      const bool staged = np > 32 && np <= SX_STAGE && nw - i - 1 > 32;
+      __syncwarp();  // the previous searches of the staged row are done
+      if (staged) {
+        for (int k = lane; k < np; k += 32) {
+          st_idx[wl][k] = aidx[sp + k];
+          st_rank[wl][k] = arank[sp + k];
+        }
+        __syncwarp();
+      }
       for (int kb = i + 1; kb < nw; kb += 32) {
         const int k = kb + lane;
         bool valid = false;
         i32 q = 0, rpq = 0;
         if (k < nw) {
           q = tw[t0 + k];
-          const int pos = lower_bound_i32(aidx, sp, ep, q);
-          if (pos < ep && aidx[pos] == q) {
-            rpq = arank[pos];
-            valid = rpq < (i32)m;
+          if (staged) {
+            const int pos = lower_bound_i32(st_idx[wl], 0, np, q);
+            if (pos < np && st_idx[wl][pos] == q) {
+              rpq = st_rank[wl][pos];
+              valid = rpq < (i32)m;
+            }
+          } else {
+            const int pos = lower_bound_i32(aidx, sp, ep, q);
+            if (pos < ep && aidx[pos] == q) {
+              rpq = arank[pos];
+              valid = rpq < (i32)m;
+            }
           }
         }
         const u32 vb = __ballot_sync(FULL, valid);
@@ -296,6 +347,136 @@ __global__ void k_cmf(const i32* __restrict__ faos, const i32* __restrict__ f0, 
       if (!skip[f]) best = max(best, face_base + f);
     }
     cmf[s] = best;
+  }
+}
+
+// ---- cofacet rows without a global sort -----------------------------------------------
+// The H1 cofacet rows are known in length before any triangle is stored: the
+// row of edge e holds every triangle containing e, one per common neighbour
+// of its ends, which the triangle count pass counts (cof_off). So the entries
+// can be scattered straight into their rows (an atomic cursor per row), and
+// only each row needs ordering: a warp sorts a row of up to 1024 entries
+// (a bitonic network in registers for <= 32, in the warp's shared memory
+// above), a block the rows up to RS_BIG entries. This replaces the stable
+// radix sort of all 3T entries by face, whose passes dominate dense batches.
+constexpr int RS_WARP_MAX = 1024;        // entries a warp sorts in shared memory
+constexpr int RS_BIG = 8192;             // entries a block sorts in shared memory
+constexpr int RS_NT = 256;
+
+__global__ void k_off_i64_to_i32(const i64* __restrict__ in, i64 n, i32* __restrict__ out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (i64)gridDim.x * blockDim.x)
+    out[i] = (i32)in[i];
+}
+
+// every triangle's rank into the rows of its three faces; a write past its
+// row's end (counts inconsistent with the triangles) is dropped and reported
+__global__ void k_cof_scatter3(const i32* __restrict__ f0, const i32* __restrict__ f1, const i32* __restrict__ f2,
+                               i64 S, i32 row_base, const i32* __restrict__ off, i32* __restrict__ cursor,
+                               i32* __restrict__ data, int* status) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (i64 s = (i64)blockIdx.x * blockDim.x + threadIdx.x; s < S; s += (i64)gridDim.x * blockDim.x) {
+    const i32 r = row_base + (i32)s;
+    const i32 f[3] = {f0[s], f1[s], f2[s]};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const i32 pos = off[f[q]] + atomicAdd(&cursor[f[q]], 1);
+      if (pos < off[f[q] + 1]) data[pos] = r;
+      else set_status(status, PH_ERR_ARG);
+    }
+  }
+}
+
+// ascending bitonic sort of n <= len2 (a power of two) values in shared memory
+// by the threads tid = 0..nthreads-1 of a group that synchronises with sync()
+template <typename Sync>
+__device__ __forceinline__ void bitonic_shared(i32* v, int len2, int tid, int nthreads, Sync sync) {
+  for (int size = 2; size <= len2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = tid; i < (len2 >> 1); i += nthreads) {
+        const int lo = 2 * i - (i & (stride - 1));  // index with bit `stride` clear
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const i32 x = v[lo], y = v[hi];
+        if ((x > y) == up) {
+          v[lo] = y;
+          v[hi] = x;
+        }
+      }
+      sync();
+    }
+  }
+}
+
+// rows of up to RS_WARP_MAX entries: one warp a row; longer rows are listed
+// (up to RS_BIG entries) for k_cof_sort_big
+__global__ void __launch_bounds__(RS_NT) k_cof_sort_rows(const i32* __restrict__ off, i64 nrows,
+                                                         i32* __restrict__ data, i32* __restrict__ big,
+                                                         int* __restrict__ nbig) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  __shared__ i32 buf[RS_NT / 32][RS_WARP_MAX];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const i64 warp = ((i64)blockIdx.x * RS_NT + threadIdx.x) >> 5;
+  const i64 nwarps = ((i64)gridDim.x * RS_NT) >> 5;
+  for (i64 r = warp; r < nrows; r += nwarps) {
+    const i32 o = off[r];
+    const int len = off[r + 1] - o;
+    if (len <= 1) continue;
+    if (len <= 32) {
+      // bitonic network across the lanes (pads sort last)
+      i32 x = lane < len ? data[o + lane] : INT_MAX;
+      for (int size = 2; size <= 32; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          const i32 y = __shfl_xor_sync(0xffffffffu, x, stride);
+          const bool up = (lane & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          x = (lower == up) ? min(x, y) : max(x, y);
+        }
+      }
+      if (lane < len) data[o + lane] = x;
+      continue;
+    }
+    if (len > RS_WARP_MAX) {
+      if (lane == 0) big[atomicAdd(nbig, 1)] = (i32)r;
+      continue;
+    }
+    int len2 = 64;
+    while (len2 < len) len2 <<= 1;
+    __syncwarp();
+    for (int i = lane; i < len2; i += 32) buf[wl][i] = i < len ? data[o + i] : INT_MAX;
+    __syncwarp();
+    bitonic_shared(buf[wl], len2, lane, 32, []() { __syncwarp(); });
+    for (int i = lane; i < len; i += 32) data[o + i] = buf[wl][i];
+    __syncwarp();
+  }
+}
+
+// the listed long rows, one block a row
+__global__ void __launch_bounds__(RS_NT) k_cof_sort_big(const i32* __restrict__ off, i32* __restrict__ data,
+                                                        const i32* __restrict__ big, const int* __restrict__ nbig,
+                                                        int* status) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  __shared__ i32 buf[RS_BIG];
+  const int nb = *nbig;
+  for (int q = blockIdx.x; q < nb; q += gridDim.x) {
+    const i32 r = big[q];
+    const i32 o = off[r];
+    const int len = off[r + 1] - o;
+    if (len > RS_BIG) {  // the caller checked the longest row; a longer one means inconsistent inputs
+      if (threadIdx.x == 0) set_status(status, PH_ERR_ARG);
+      continue;
+    }
+    int len2 = 2 * RS_WARP_MAX;
+    while (len2 < len) len2 <<= 1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < len2; i += RS_NT) buf[i] = i < len ? data[o + i] : INT_MAX;
+    __syncthreads();
+    bitonic_shared(buf, len2, threadIdx.x, RS_NT, []() { __syncthreads(); });
+    for (int i = threadIdx.x; i < len; i += RS_NT) data[o + i] = buf[i];
   }
 }
 
@@ -498,6 +679,71 @@ extern "C" int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const
   PH_TRY(radix_sort_pairs(keys, vals, H, 0, std::min(32, ((fb + 7) / 8) * 8), rws, radix_sort_workspace_bytes(H), s));
   ph::count_launch();
   ph::launch_pdl(k_cof_fill, dim3(grid_for(H)), dim3(256), 0, s, keys, vals, H, n_faces, cof_off, cof_data);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int32_t ph_cofacet_rows3_max_row(void) { return RS_BIG; }
+
+extern "C" size_t ph_cofacet_rows3_workspace_bytes(int64_t n_faces) {
+  return Carve::need(sizeof(i32) * (size_t)std::max<i64>(n_faces, 1)) * 2 + Carve::need(sizeof(int));
+}
+
+extern "C" int ph_cofacet_rows3(const int32_t* f0, const int32_t* f1, const int32_t* f2, int64_t S, int64_t n_faces,
+                                int32_t row_base, const int64_t* row_off, int32_t max_row, int32_t* cof_off,
+                                int32_t* cof_data, int* d_status, void* workspace, size_t workspace_bytes,
+                                void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (S < 0 || n_faces < 0 || !row_off || !cof_off || 3 * S >= (int64_t(1) << 31)) return PH_ERR_ARG;
+  if (max_row > RS_BIG) {
+    record_message("ph_cofacet_rows3: a row exceeds the in-shared-memory sort; use ph_cofacet_csr");
+    return PH_ERR_ARG;
+  }
+  Carve c(workspace, workspace_bytes);
+  i32* cursor = c.take<i32>(std::max<i64>(n_faces, 1));
+  i32* big = c.take<i32>(std::max<i64>(n_faces, 1));
+  int* nbig = c.take<int>(1);
+  if (!cursor || !big || !nbig) return PH_ERR_ARG;
+  ph::count_launch();
+  ph::launch_pdl(k_off_i64_to_i32, dim3(grid_for(n_faces + 1)), dim3(256), 0, s, row_off, n_faces, cof_off);
+  if (S == 0 || n_faces == 0) {
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  ph::zero_async(cursor, sizeof(i32) * n_faces, s, nbig, sizeof(int));
+  ph::count_launch();
+  ph::launch_pdl(k_cof_scatter3, dim3(grid_for(S)), dim3(256), 0, s, f0, f1, f2, S, row_base, (const i32*)cof_off,
+                 cursor, cof_data, d_status);
+  const int gw = (int)std::max<i64>(1, std::min<i64>((n_faces + RS_NT / 32 - 1) / (RS_NT / 32), 148 * 16));
+  ph::count_launch();
+  ph::launch_pdl(k_cof_sort_rows, dim3(gw), dim3(RS_NT), 0, s, (const i32*)cof_off, n_faces, cof_data, big, nbig);
+  ph::count_launch();
+  ph::launch_pdl(k_cof_sort_big, dim3(148 * 2), dim3(RS_NT), 0, s, (const i32*)cof_off, cof_data, (const i32*)big,
+                 (const int*)nbig, d_status);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+// the largest per-item count given by an exclusive scan: out = max(off[i+1] - off[i])
+__global__ void k_max_diff(const i64* __restrict__ off, i64 n, i64* __restrict__ out) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  i64 m = 0;
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    m = max(m, off[i + 1] - off[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)m);
+}
+
+extern "C" int ph_max_count(const int64_t* off, int64_t n, int64_t* d_out, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n < 0 || !off || !d_out) return PH_ERR_ARG;
+  ph::zero_async(d_out, sizeof(int64_t), s);
+  if (n > 0) {
+    ph::count_launch();
+    ph::launch_pdl(k_max_diff, dim3((unsigned)std::max<i64>(1, std::min<i64>((n + 255) / 256, 148 * 8))), dim3(256), 0,
+                   s, off, n, d_out);
+  }
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

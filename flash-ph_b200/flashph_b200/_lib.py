@@ -92,6 +92,10 @@ _SIGS = {
     "ph_cofacet_csr_workspace_bytes": (SZ, [I64, I32]),
     "ph_cofacet_csr": (ctypes.c_int, [P, P, P, P, I32, I64, I64, I32, P, P, P, SZ, P]),
     "ph_cof_max_face": (ctypes.c_int, [P, P, P, P, I32, I64, I32, P, P, P]),
+    "ph_cofacet_rows3_max_row": (I32, []),
+    "ph_cofacet_rows3_workspace_bytes": (SZ, [I64]),
+    "ph_cofacet_rows3": (ctypes.c_int, [P, P, P, I64, I64, I32, P, I32, P, P, P, P, SZ, P]),
+    "ph_max_count": (ctypes.c_int, [P, I64, P, P]),
     "ph_reduce_workspace_bytes": (SZ, [I64, I64, I64]),
     "ph_reduce": (ctypes.c_int, [P, P, I64, I32, I64, I32, I64, P, P, P, P, P, I64, P, P, P, SZ, P]),
     "ph_mark_pivots": (ctypes.c_int, [P, P, I64, I32, P, I64, P]),

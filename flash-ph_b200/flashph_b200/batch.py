@@ -389,7 +389,7 @@ def _native_chunk(pts: list[Tensor], ts: list[float], dims: list[int], device, m
     d = np.array([p.shape[1] for p in pts], dtype=np.int32)
     t = np.array(ts, dtype=np.float64)
     md = np.array(dims, dtype=np.int32)
-    mode = _EDGE_MODES.get(os.environ.get("FLASHPH_EDGE_SCREEN", "auto").lower(), 0)
+    mode = _edge_mode(pts, ts, n, d, device)
     s = L.stream_handle(device)
     res = ctypes.c_void_p()
     rc = lib.ph_rips_persistence_batch(ptrs, n.ctypes.data, d.ctypes.data, t.ctypes.data, md.ctypes.data, k,
@@ -423,6 +423,33 @@ def _native_chunk(pts: list[Tensor], ts: list[float], dims: list[int], device, m
     finally:
         lib.ph_batch_result_free(res)
     return out
+
+
+def _edge_mode(pts: list[Tensor], ts: list[float], n: np.ndarray, d: np.ndarray, device) -> int:
+    """The chunk's edge kernel: FLASHPH_EDGE_SCREEN=on / off, else the
+    autotuner's choice for the chunk's (largest d, mean cloud size) key (one
+    timed trial of both kernels on the first chunk of each key)."""
+    env = os.environ.get("FLASHPH_EDGE_SCREEN", "auto").lower()
+    if env in ("on", "off"):
+        return _EDGE_MODES[env]
+    from . import autotune
+    from ._edges import enumerate_segments
+
+    key_segs = np.zeros(len(pts), dtype=SEG_DTYPE)
+    key_segs["n"] = n
+    key_segs["d"] = d
+    state = {}
+
+    def trial(screen: bool) -> int:
+        if "b" not in state:  # the chunk's union layout, built only when a trial runs
+            state["b"] = _Batch(pts, ts, [0] * len(pts), device)
+        b = state["b"]
+        pairs = sum(int(x) * (int(x) - 1) // 2 for x in n)
+        cap = int(min(pairs, max(1 << 20, 256 * b.N)))
+        ei, _, _ = enumerate_segments(b.pts, b.segs_np, b.segs, b.ntiles, cap, screen=screen)
+        return int(ei.numel())
+
+    return autotune.choose(key_segs, trial)
 
 
 def _repack(chunk: list[int], counts: list[int], edges: list[int]) -> list[list[int]]:

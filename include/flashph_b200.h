@@ -274,6 +274,26 @@ int ph_cofacet_csr(const int32_t* faces_aos, const int32_t* f0, const int32_t* f
                    int32_t* cof_off, int32_t* cof_data, void* workspace, size_t workspace_bytes,
                    void* stream);
 
+/* The H1 cofacet CSR of ph_cofacet_csr (k = 3, faces f0/f1/f2 per triangle)
+ * without its sort: row_off (n_faces + 1, int64) are the rows' offsets known
+ * beforehand -- the cofacet offsets ph_triangles_count writes (one entry per
+ * common neighbour of an edge's ends), masked like the triangles when some
+ * are cleared -- so every triangle's rank is scattered straight into its
+ * three rows and each row is then sorted in shared memory (a warp a row up to
+ * 1024 entries, a block a row up to ph_cofacet_rows3_max_row()). max_row:
+ * the longest row (ph_max_count on row_off); longer rows return PH_ERR_ARG
+ * (use ph_cofacet_csr). Same output as ph_cofacet_csr; replaces the same
+ * reduce_h1_gpu.py:107 _build_cofacet_csr_h1. d_status gets PH_ERR_ARG if a
+ * row turns out longer than max_row. */
+int32_t ph_cofacet_rows3_max_row(void);
+size_t ph_cofacet_rows3_workspace_bytes(int64_t n_faces);
+int ph_cofacet_rows3(const int32_t* f0, const int32_t* f1, const int32_t* f2, int64_t S, int64_t n_faces,
+                     int32_t row_base, const int64_t* row_off, int32_t max_row, int32_t* cof_off, int32_t* cof_data,
+                     int* d_status, void* workspace, size_t workspace_bytes, void* stream);
+/* *d_out = max over i < n of off[i + 1] - off[i] (int64, device): the longest
+ * row of an exclusive-scan offset array. Bookkeeping with no counterpart. */
+int ph_max_count(const int64_t* off, int64_t n, int64_t* d_out, void* stream);
+
 /* For every simplex: the largest global rank (face_base + face index) among
  * its faces that are not skipped, -1 if all are skipped. This is the
  * cofacet_max_face of reduce_h1_gpu.py:186-197 / cohomology_general.py:50-61. */

@@ -154,3 +154,50 @@ def test_h0_rows_through_both_scan_forms(E):
     assert np.all(rows[:, 0] == 0)
     assert np.array_equal(rows[:k, 1], filt[mask == 1])
     assert np.all(np.isinf(rows[k:, 1]))
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_cofacet_rows_without_sort_equal_the_sorted_csr(seed):
+    """ph_cofacet_rows3 (entries scattered into rows whose lengths are known,
+    then each row sorted in shared memory) against ph_cofacet_csr (stable
+    radix sort by face), on triangles with random faces and a few hub faces
+    in thousands of triangles (rows sorted by a warp, by a block, and rows of
+    one entry); identical offsets and rows, and the longest row reported."""
+    from flashph_b200 import _lib as L
+    rng = np.random.default_rng(seed)
+    E, T = 6000, 60000
+    f = rng.integers(0, E, size=(T, 3)).astype(np.int32)
+    hubs = np.array([7, 4000, 5999], dtype=np.int32)
+    for h, cnt in zip(hubs, (3000, 1500, 40)):
+        idx = rng.choice(T, size=cnt, replace=False)
+        f[idx, rng.integers(0, 3, size=cnt)] = h
+    f0, f1, f2 = (torch.from_numpy(np.ascontiguousarray(f[:, q])).cuda() for q in range(3))
+    counts = np.bincount(f.reshape(-1), minlength=E).astype(np.int64)
+    off = np.zeros(E + 1, dtype=np.int64)
+    off[1:] = np.cumsum(counts)
+    off_d = torch.from_numpy(off).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    mx = torch.zeros(1, dtype=torch.int64, device="cuda")
+    L.call("ph_max_count", off_d.data_ptr(), E, mx.data_ptr(), s)
+    assert int(mx.item()) == int(counts.max()) > 2048
+    want_off = torch.empty(E + 1, dtype=torch.int32, device="cuda")
+    want = torch.empty(3 * T, dtype=torch.int32, device="cuda")
+    nb = L.query("ph_cofacet_csr_workspace_bytes", T, 3)
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    L.call("ph_cofacet_csr", None, f0.data_ptr(), f1.data_ptr(), f2.data_ptr(), 3, T, E, 100000,
+           want_off.data_ptr(), want.data_ptr(), ws.data_ptr(), nb, s)
+    got_off = torch.empty(E + 1, dtype=torch.int32, device="cuda")
+    got = torch.empty(3 * T, dtype=torch.int32, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nb3 = L.query("ph_cofacet_rows3_workspace_bytes", E)
+    ws3 = torch.empty(nb3, dtype=torch.uint8, device="cuda")
+    L.call("ph_cofacet_rows3", f0.data_ptr(), f1.data_ptr(), f2.data_ptr(), T, E, 100000, off_d.data_ptr(),
+           int(mx.item()), got_off.data_ptr(), got.data_ptr(), st.data_ptr(), ws3.data_ptr(), nb3, s)
+    assert int(st.item()) == 0
+    assert torch.equal(got_off, want_off)
+    assert torch.equal(got, want)
+    # a longest row beyond the in-shared-memory sort is refused before any work
+    too_long = int(L.lib().ph_cofacet_rows3_max_row()) + 1
+    rc = L.lib().ph_cofacet_rows3(f0.data_ptr(), f1.data_ptr(), f2.data_ptr(), T, E, 100000, off_d.data_ptr(),
+                                  too_long, got_off.data_ptr(), got.data_ptr(), st.data_ptr(), ws3.data_ptr(), nb3, s)
+    assert rc == 2
