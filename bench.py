@@ -800,6 +800,35 @@ def rooflines(stages, edge_ms, n, d, E, T, pk, src):
     return out
 
 
+def l2_hop_ns(dev, mib=64, hops=200_000, seed=3):
+    """Nanoseconds of one dependent L2 load: a single thread chasing a random
+    cycle through a 64 MiB buffer (it fits the 126 MB L2), median of 3 laps."""
+    import torch
+    from flashph_b200 import _lib as L
+    n = (mib << 20) // 4
+    perm = np.random.default_rng(seed).permutation(n).astype(np.uint32)
+    nxt = np.empty(n, dtype=np.uint32)
+    nxt[perm] = np.roll(perm, -1)  # one cycle through every entry
+    d = torch.from_numpy(nxt.view(np.int32)).to(dev)
+    out = torch.zeros(2, dtype=torch.int64, device=dev)
+    laps = []
+    for _ in range(3):
+        L.call("ph_probe_l2_chase", d.data_ptr(), hops, int(perm[0]), out.data_ptr(), L.stream_handle(dev))
+        laps.append(float(out[0].item()) / hops)
+    return statistics.median(laps)
+
+
+def latency_roofline(stage_ms, crit_path, hop_ns):
+    """The H1 reduction against its latency bound: the oracle's critical path
+    (the longest chain of dependent column additions) times two dependent L2
+    loads per addition (the pivot's owner word, then the owning record)."""
+    min_ms = crit_path * 2 * hop_ns * 1e-6
+    return {"kernel": "k_reduce (H1, with classify/finish/rows)", "bound": "latency",
+            "crit_path": int(crit_path), "dependent_l2_loads_per_step": 2, "l2_hop_ns": round(hop_ns, 1),
+            "min_ms": round(min_ms, 4), "achieved_ms": round(stage_ms, 4), "frac": round(min_ms / stage_ms, 4),
+            "per_unit": "crit_path x 2 x measured dependent L2 load latency (one-thread pointer chase, 64 MiB)"}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -971,8 +1000,10 @@ def main():
             oracle.build()
             cores = os.cpu_count() or 1
             t0 = time.perf_counter()
-            oracle.run(pts_np, THRESH, MAX_DIM, fused=True, nthreads=cores)
+            ref = oracle.run(pts_np, THRESH, MAX_DIM, fused=True, nthreads=cores)
             cpu_ms = (time.perf_counter() - t0) * 1e3
+            if "h1.reduce" in stage_ms:
+                rl["h1.reduce.latency"] = latency_roofline(stage_ms["h1.reduce"], ref["crit_path"], l2_hop_ns(dev))
             cpu = {"value": round(cpu_ms, 2), "unit": "ms", "cores": cores, "kind": "port",
                    "sample": "one run of the full workload (C++ port of the reference algorithm)"}
         rows = [int(o.shape[0]) for o in out]

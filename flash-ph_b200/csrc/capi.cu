@@ -127,3 +127,35 @@ extern "C" void ph_set_reduce_limits(int64_t max_steps, int64_t first_pool_entri
   ph::g_reduce_max_steps.store(max_steps > 0 ? max_steps : 0, std::memory_order_relaxed);
   ph::g_reduce_first_pool.store(first_pool_entries > 0 ? first_pool_entries : 0, std::memory_order_relaxed);
 }
+
+// ---- a measurement probe: the latency of one dependent L2 load ------------------------
+namespace {
+// One thread follows a chain of indices through `next` (a random cycle over a
+// buffer that fits L2): every load's address depends on the previous load, as
+// the reducer's owner-word and record loads do. A first lap over the same
+// addresses warms L2; the second is timed.
+__global__ void k_chase(const uint32_t* __restrict__ next, int hops, uint32_t start, unsigned long long* out) {
+  uint32_t w = start;
+  for (int i = 0; i < hops; ++i) w = __ldcg(next + w);
+  uint32_t p = start;
+  unsigned long long t0, t1;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0)::"memory");
+  for (int i = 0; i < hops; ++i) p = __ldcg(next + p);
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1)::"memory");
+  out[0] = t1 - t0;
+  out[1] = (unsigned long long)p + w;  // keeps both chains live
+}
+}  // namespace
+
+extern "C" int ph_probe_l2_chase(const uint32_t* next, int32_t hops, uint32_t start, unsigned long long* d_out,
+                                 void* stream) {
+  if (!next || !d_out || hops < 1) return PH_ERR_ARG;
+  ph::count_launch();
+  k_chase<<<1, 1, 0, (cudaStream_t)stream>>>(next, hops, start, d_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    ph::record_error(e);
+    return PH_ERR_CUDA;
+  }
+  return PH_OK;
+}

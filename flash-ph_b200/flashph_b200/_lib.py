@@ -59,6 +59,7 @@ _SIGS = {
     "ph_result_copy_all": (ctypes.c_int, [P, P, I32, P]),
     "ph_set_dependent_launch": (None, [I32]),
     "ph_set_reduce_limits": (None, [I64, I64]),
+    "ph_probe_l2_chase": (ctypes.c_int, [P, I32, ctypes.c_uint32, P, P]),
     "ph_triangles_total_edges_workspace_bytes": (SZ, [I64, I64]),
     "ph_triangles_total_edges": (ctypes.c_int, [P, P, I64, I64, P, P, SZ, P]),
     "ph_result_free": (None, [P]),

@@ -63,6 +63,15 @@ void ph_set_dependent_launch(int32_t enable);
  * without a device fault. */
 void ph_set_reduce_limits(int64_t max_steps, int64_t first_pool_entries);
 
+/* Measurement probe: one thread follows `hops` links of the cycle `next`
+ * (next[i] is the index of the next entry; a random cycle over a buffer that
+ * fits L2) from `start`, once to warm L2 and once timed; d_out[0] receives
+ * the timed lap's nanoseconds (device memory, 2 entries). The latency of one
+ * dependent L2 load, the unit of the reduction's latency bound. No
+ * counterpart in the reference. */
+int ph_probe_l2_chase(const uint32_t* next, int32_t hops, uint32_t start, unsigned long long* d_out,
+                      void* stream);
+
 /* ---- filtration -------------------------------------------------------- */
 
 /* One point cloud of a batch. A batch is the disjoint union of its clouds:
