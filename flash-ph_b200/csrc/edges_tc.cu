@@ -629,10 +629,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const u32 idesc = it.nh() == 2 ? idesc2 : idesc1;
         const u64 da0 = umma_desc(smem_u32(sA + as * sh.a_bytes), sh.layout, sh.sbo);
         const u64 db0 = umma_desc(smem_u32(sB + bs * sh.b_bytes), sh.layout, sh.sbo);
-        for (int s = 0; s < ks; ++s) {
-          const u64 atom = (u64)(s / spa), sub = (u64)((s % spa) * 2);
-          umma_bf16(tmem + (u32)ts * stage_cols, da0 + atom * a_step + sub, db0 + atom * b_step + sub, idesc,
-                    s > 0 ? 1u : 0u);
+        // K slice s sits in swizzle atom s / spa at 32-byte step s % spa, kept
+        // incrementally: a division per MMA on this one thread cost more than
+        // the MMA itself
+        u64 da = da0, db = db0;
+        for (int s = 0, sub = 0; s < ks; ++s) {
+          umma_bf16(tmem + (u32)ts * stage_cols, da, db, idesc, s > 0 ? 1u : 0u);
+          if (++sub == spa) {
+            sub = 0;
+            da += a_step - (u64)(2 * (spa - 1));
+            db += b_step - (u64)(2 * (spa - 1));
+          } else {
+            da += 2;
+            db += 2;
+          }
         }
         umma_commit(bar(BAR_BE + bs));
         umma_commit(bar(BAR_TF + ts));
@@ -659,6 +669,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     unsigned long long n_cand = 0, n_forced = 0;
     int cnt = 0;
     ph_cloud_seg qs{};  // cloud of the queued candidates
+    float sqthr = 0.0f;  // sqrt of the widened threshold of that cloud, rounded up
     auto flush = [&]() {
       flush_queue(queue, cnt, qs, pts_all, oi, oj, od, cap, count);
       n_cand += (unsigned long long)cnt;
@@ -669,24 +680,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (g == 1 && T > 1) it.next();
     for (i64 t = g; t < T; t += 2) {
       const ph_cloud_seg& sg = it.sg;
-      if (cnt && (sg.pt_off != qs.pt_off || sg.vbase != qs.vbase)) flush();
+      const bool new_cloud = sg.pt_off != qs.pt_off || sg.vbase != qs.vbase || t == g;
+      if (cnt && new_cloud) flush();
       qs = sg;
       const int nh = it.nh();
       const i64 i0 = it.I * TC_T, j0 = it.J * TC_T;
-      // widened thresholds of the item's column blocks, computed while the MMAs run
-      const double rt = sqrt((double)sg.thr_sq * thr_scale) + (double)blkrad[it.blk + it.I];
+      // widened thresholds of the item's column blocks, computed while the MMAs
+      // run: (sqrt(thr') + r_I + r_J)^2 (1 + 2^-20) + 2^-96 with every FP32
+      // operation rounded up (an upper bound of that value; the square root,
+      // in FP64, once per cloud)
+      if (new_cloud) sqthr = __double2float_ru(sqrt((double)sg.thr_sq * thr_scale));
+      const float rt = __fadd_ru(sqthr, blkrad[it.blk + it.I]);
       float base[2];
       bool force[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const double radius = rt + (h < nh ? (double)blkrad[it.blk + it.J + h] : 0.0);
-        const double base_d = radius * radius * (1.0 + 0x1p-20) + 0x1p-96;
-        force[h] = !(base_d < 3.0e38);
-        base[h] = force[h] ? 0.0f : __double2float_ru(base_d);
+        const float radius = __fadd_ru(rt, h < nh ? blkrad[it.blk + it.J + h] : 0.0f);
+        const float b = __fadd_ru(__fmul_ru(__fmul_ru(radius, radius), 1.0f + 0x1p-20f), 0x1p-96f);
+        force[h] = !(b < 3.0e38f);
+        base[h] = force[h] ? 0.0f : b;
       }
       // one compare per pair into a lane mask; the set bits are queued one per
       // lane per round (a round per candidate in the densest lane)
-      auto screen = [&](const u32 (&v)[32], int c0, float bs_) {
+      // the smallest of a lane's 32 values (a min tree)
+      auto vmin = [](const u32 (&v)[32]) {
         float m16[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) m16[k] = fminf(__uint_as_float(v[k]), __uint_as_float(v[k + 16]));
@@ -694,7 +711,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int w = 8; w > 0; w >>= 1)
 #pragma unroll
           for (int k = 0; k < w; ++k) m16[k] = fminf(m16[k], m16[k + w]);
-        if (!__any_sync(FULL, m16[0] < bs_)) return;
+        return m16[0];
+      };
+      // the candidates among a lane's 32 values, queued
+      auto screen = [&](const u32 (&v)[32], int c0, float bs_) {
         u32 mask = 0;
 #pragma unroll
         for (int k = 0; k < 32; ++k) mask |= (__uint_as_float(v[k]) < bs_ ? 1u : 0u) << k;
@@ -728,6 +748,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         tmem_ld32_issue(taddr + (u32)c0, v0);
         tmem_ld32_issue(taddr + (u32)(c0 + 32), v1);
         tmem_ld_wait();
+        // both min trees before one vote: independent chains side by side and
+        // one branch per 64 columns (almost always: no candidate)
+        const float mn = fminf(vmin(v0), vmin(v1));
+        if (!__any_sync(FULL, mn < base[h])) continue;
         screen(v0, c0, base[h]);
         screen(v1, c0 + 32, base[h]);
       }
