@@ -454,7 +454,7 @@ __device__ __forceinline__ void emit_warp(bool emit, i64 gi, i64 gj, float acc, 
 // Exact chain for the first cnt queued cloud-local pairs of cloud qs, 32 at a
 // time with warp-aggregated emission. Kept out of line: the screening loop
 // around its call sites must stay small.
-__device__ __noinline__ void flush_queue(const uint2* __restrict__ queue, int cnt, const ph_cloud_seg& qs,
+__device__ __noinline__ void flush_queue(const uint2* __restrict__ queue, int cnt, const ph_cloud_seg qs,
                                          const float* __restrict__ pts_all, i32* __restrict__ oi,
                                          i32* __restrict__ oj, float* __restrict__ od, i64 cap,
                                          unsigned long long* __restrict__ count) {
