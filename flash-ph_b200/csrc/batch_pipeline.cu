@@ -125,6 +125,26 @@ __global__ void k_masked_counts(const int64_t* __restrict__ off, i64 E, const ui
     cnt[e] = keep[e] ? (i32)(off[e + 1] - off[e]) : 0;
 }
 
+// Clouds that may hold more than max_triangles triangles: a graph with m
+// edges has at most sqrt(2)/3 m^1.5 of them, so only clouds with more than
+// m_star edges are counted exactly before the per-edge pass.
+__global__ void k_tri_want(const int64_t* __restrict__ e_off, int K, i64 m_star, uint8_t* __restrict__ want) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < K; c += gridDim.x * blockDim.x)
+    want[c] = (uint8_t)(e_off[c + 1] - e_off[c] > m_star);
+}
+
+// the clouds whose triangles the per-edge pass counts: all but those counted
+// exactly and over the limit
+__global__ void k_tri_keep(const uint8_t* __restrict__ want, const unsigned long long* __restrict__ tot, int K,
+                           i64 max_t, uint8_t* __restrict__ keep) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < K; c += gridDim.x * blockDim.x)
+    keep[c] = (uint8_t)!(want[c] && tot[c] > (unsigned long long)max_t);
+}
+
 inline int grid_for(i64 n, int nt = 256) {
   return (int)std::max<i64>(1, std::min<i64>((n + nt - 1) / nt, 148 * 16));
 }
@@ -326,12 +346,14 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
   for (int c = 0; c <= K; ++c) res->off[0][c] = c < K ? segs[c].vbase : N;
 
   // per-cloud host arrays read back in bulk: [0, K] edge offsets, then K counts
-  PinnedLease hb(sizeof(int64_t) * (4 * (size_t)K + 8) + 256);
+  PinnedLease hb(sizeof(int64_t) * (6 * (size_t)K + 8) + 256);
   if (!hb.p.host) return give_up(fail(PH_ERR_CUDA, "ph_rips_persistence_batch: pinned host buffer unavailable"));
   int64_t* hcnt = hb.as<int64_t>();            // 16 words of cnt
   int64_t* hoff = hcnt + 16;                  // K + 1 offsets
   int64_t* hper = hoff + (K + 1);             // K per-cloud counts
   int64_t* hoff2 = hper + K;                  // K + 1 more offsets
+  int64_t* htot = hoff2 + (K + 1);            // K exact totals of the clouds that may be over the limit
+  uint8_t* hwant = reinterpret_cast<uint8_t*>(htot + K);  // K flags: which clouds those are
 
   if (dim_all == 0) {
     Part parts[2] = {{cnt, hcnt, 16 * sizeof(int64_t)}, {e_off, hoff, sizeof(int64_t) * (K + 1)}};
@@ -352,18 +374,43 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
   uint8_t* eflag = A.take<uint8_t>(E);
   const size_t tc_b = ph_triangles_count_workspace_bytes(E);
   void* tc_ws = A.bytes(tc_b);
+  // clouds that may be over max_triangles are counted exactly first (the
+  // bitmap total: far cheaper than the per-edge pass on a dense cloud), and
+  // the per-edge pass skips those over it
+  uint8_t* want = A.take<uint8_t>(K);
+  uint8_t* tkeep = A.take<uint8_t>(K);
+  unsigned long long* ttot = A.take<unsigned long long>(K);
+  int* tnext = A.take<int>(1);
   if (A.failed) return alloc_fail();
-  PH_TRY(ph_triangles_count(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b, s));
+  const bool pre = max_triangles > 0 && E > 0 && N <= ph_triangles_total_max_vertices();
+  if (pre) {
+    const double bound_m = std::pow(3.0 * (double)max_triangles / std::sqrt(2.0), 2.0 / 3.0);
+    const i64 m_star = std::max<i64>(0, (i64)std::floor(bound_m) - 1);  // conservative: a few more clouds counted
+    count_launch();
+    ph::launch_pdl(k_tri_want, dim3(grid_for(K)), dim3(256), 0, s, (const int64_t*)e_off, K, m_star, want);
+    PH_TRY(ph_batch_triangles_total(adj_ptr, adj_idx, N, vcloud, want, K, ttot, tnext, s));
+    count_launch();
+    ph::launch_pdl(k_tri_keep, dim3(grid_for(K)), dim3(256), 0, s, (const uint8_t*)want,
+                   (const unsigned long long*)ttot, K, (i64)max_triangles, tkeep);
+  }
+  PH_TRY(triangles_count_masked(si, sj, E, adj_ptr, adj_idx, adj_rank, tri_off, tcof_off, tc_ws, tc_b,
+                                pre ? tkeep : nullptr, pre ? vcloud : nullptr, s));
   PH_TRY(ph_max_count(tcof_off, E, cnt + 8, s));  // the longest cofacet row (before any clearing: a bound)
   count_launch();
   ph::launch_pdl(k_seg_diff, dim3(grid_for(K)), dim3(256), 0, s, (const int64_t*)tri_off, (const int64_t*)e_off, K,
                  per);
   {
-    Part parts[3] = {{cnt, hcnt, 16 * sizeof(int64_t)},
+    Part parts[5] = {{cnt, hcnt, 16 * sizeof(int64_t)},
                      {e_off, hoff, sizeof(int64_t) * (K + 1)},
-                     {per, hper, sizeof(int64_t) * K}};
-    if (readback_parts(parts, 3, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
+                     {per, hper, sizeof(int64_t) * K},
+                     {ttot, htot, sizeof(int64_t) * K},
+                     {want, hwant, (size_t)K}};
+    if (readback_parts(parts, pre ? 5 : 3, slots, s) != PH_OK) return give_up(PH_ERR_CUDA);
   }
+  // a cloud counted exactly and over the limit counted nothing in the per-edge pass
+  if (pre)
+    for (int c = 0; c < K; ++c)
+      if (hwant[c] && htot[c] > max_triangles) hper[c] = htot[c];
   if ((int)(hcnt[1] >> 32) != 0) return give_up(fail((int)(hcnt[1] >> 32), "ph_boruvka_mst failed"));
   std::vector<uint8_t> keep1(K, 0), keep2(K, 0);
   i64 T = 0, span1 = 0;

@@ -41,6 +41,11 @@ void count_launch();
 // The reducer's step cap per column (ph_set_reduce_limits; 2^24 by default)
 // and the cap on a native call's first reduction pool (0: none).
 long long reduce_max_steps();
+// the triangle count pass with an optional per-cloud mask (simplices.cu)
+int triangles_count_masked(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int32_t* adj_ptr,
+                           const int32_t* adj_idx, const int32_t* adj_rank, int64_t* tri_off, int64_t* cof_off,
+                           void* workspace, size_t workspace_bytes, const uint8_t* keep, const int32_t* vcloud,
+                           cudaStream_t s);
 long long reduce_first_pool_limit();
 
 // Raises a kernel's dynamic shared memory limit to the device's opt-in

@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
                                                     i32* __restrict__ tri_cnt, i32* __restrict__ cof_cnt,
                                                     const i64* __restrict__ tri_off, i32* __restrict__ tm,
                                                     i32* __restrict__ tw, i32* __restrict__ tfa,
-                                                    i32* __restrict__ tfb) {
+                                                    i32* __restrict__ tfb, const uint8_t* __restrict__ keep,
+                                                    const i32* __restrict__ vcloud) {
   ph::pdl_wait();
   ph::pdl_trigger();
   __shared__ i32 st_idx[SX_WARPS][SX_STAGE];
@@ -65,6 +66,14 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
   for (i64 m = warp; m < E; m += nwarps) {
     __syncwarp();  // the previous edge's searches of the staged row are done
     const i32 a = ei[m], b = ej[m];
+    // a batch's count pass: the edges of a cloud already over its limit count nothing
+    if (keep && !keep[vcloud[a]]) {
+      if (!EMIT && lane == 0) {
+        tri_cnt[m] = 0;
+        cof_cnt[m] = 0;
+      }
+      continue;
+    }
     int sa = aptr[a], ea = aptr[a + 1], sb = aptr[b], eb = aptr[b + 1];
     // walk the shorter row, search the longer
     const bool a_short = (ea - sa) <= (eb - sb);
@@ -139,10 +148,16 @@ __global__ void __launch_bounds__(SX_NT) k_triangles(const i32* __restrict__ ei,
 // UPPER: the rows hold only the larger neighbours, in any order (the upper
 // adjacency of k_upper_fill), so no row is searched; otherwise the rows are
 // the full adjacency sorted by neighbour.
-template <bool UPPER>
+// SEG: per-cloud totals of a batch's union graph: vertex a counts into
+// per[vcloud[a]], and only the vertices of clouds with want[cloud] set are
+// visited (total unused).
+template <bool UPPER, bool SEG = false>
 __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ aptr, const i32* __restrict__ aidx,
                                                     i64 n, int* __restrict__ next,
-                                                    unsigned long long* __restrict__ total) {
+                                                    unsigned long long* __restrict__ total,
+                                                    const i32* __restrict__ vcloud = nullptr,
+                                                    const uint8_t* __restrict__ want = nullptr,
+                                                    unsigned long long* __restrict__ per = nullptr) {
   ph::pdl_wait();
   ph::pdl_trigger();
   extern __shared__ u32 nbits[];
@@ -157,6 +172,7 @@ __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ apt
     __syncthreads();
     const i64 a = cur;
     if (a >= n) break;
+    if (SEG && !want[vcloud[a]]) continue;
     const int s = aptr[a], e = aptr[a + 1];
     if (e - s < 2) continue;
     for (int p = s + threadIdx.x; p < e; p += SX_NT) {
@@ -179,7 +195,13 @@ __global__ void __launch_bounds__(SX_NT) k_tri_total(const i32* __restrict__ apt
       const i32 v = aidx[p];
       nbits[v >> 5] = 0u;
     }
+    if (SEG) {  // this vertex's triangles to its cloud
+      for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
+      if (lane == 0 && cnt) atomicAdd(per + vcloud[a], cnt);
+      cnt = 0;
+    }
   }
+  if (SEG) return;
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(FULL, cnt, o);
   if (lane == 0 && cnt) atomicAdd(total, cnt);
 }
@@ -500,7 +522,16 @@ extern "C" int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, 
                                   const int32_t* adj_ptr, const int32_t* adj_idx, const int32_t* adj_rank,
                                   int64_t* tri_off, int64_t* cof_off, void* workspace,
                                   size_t workspace_bytes, void* stream) {
-  cudaStream_t s = (cudaStream_t)stream;
+  return ph::triangles_count_masked(edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, tri_off, cof_off, workspace,
+                                    workspace_bytes, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+// The count pass with an optional per-cloud mask (keep[vcloud[i]] == 0: the
+// edge counts nothing), for a batch whose over-limit clouds are known first.
+int ph::triangles_count_masked(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int32_t* adj_ptr,
+                               const int32_t* adj_idx, const int32_t* adj_rank, int64_t* tri_off, int64_t* cof_off,
+                               void* workspace, size_t workspace_bytes, const uint8_t* keep, const int32_t* vcloud,
+                               cudaStream_t s) {
   if (E < 0) return PH_ERR_ARG;
   Carve c(workspace, workspace_bytes);
   i32* tc = c.take<i32>(E + 1);
@@ -510,7 +541,7 @@ extern "C" int ph_triangles_count(const int32_t* edge_i, const int32_t* edge_j, 
   if (E > 0) {
     ph::count_launch();
     ph::launch_pdl(k_triangles<false>, dim3(warp_grid(E)), dim3(SX_NT), 0, s, edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, tc, cc,
-                                                      nullptr, nullptr, nullptr, nullptr, nullptr);
+                                                      nullptr, nullptr, nullptr, nullptr, nullptr, keep, vcloud);
   }
   PH_TRY(scan_exclusive_i32_i64(tc, tri_off, E, sws, scan_workspace_bytes(E), s));
   PH_TRY(scan_exclusive_i32_i64(cc, cof_off, E, sws, scan_workspace_bytes(E), s));
@@ -542,7 +573,37 @@ extern "C" int ph_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx
   const int occ = ph::occupancy((const void*)k_tri_total<false>, SX_NT, smem);
   const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
   ph::count_launch();
-  ph::launch_pdl(k_tri_total<false>, dim3(grid), dim3(SX_NT), smem, s, adj_ptr, adj_idx, n, d_next, d_total);
+  ph::launch_pdl(k_tri_total<false>, dim3(grid), dim3(SX_NT), smem, s, adj_ptr, adj_idx, n, d_next, d_total,
+                 (const i32*)nullptr, (const uint8_t*)nullptr, (unsigned long long*)nullptr);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+
+extern "C" int ph_batch_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx, int64_t n,
+                                        const int32_t* vcloud, const uint8_t* want, int32_t nclouds,
+                                        unsigned long long* d_per, int* d_next, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n < 0 || nclouds < 1 || !adj_ptr || !vcloud || !want || !d_per || !d_next) return PH_ERR_ARG;
+  if (n > ph_triangles_total_max_vertices()) {
+    record_message("ph_batch_triangles_total: n exceeds the shared-memory bitmap (1638400 vertices)");
+    return PH_ERR_ARG;
+  }
+  ph::zero_async(d_per, sizeof(unsigned long long) * (size_t)nclouds, s, d_next, sizeof(int));
+  if (n < 3) {
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  const size_t smem = (size_t)((n + 31) / 32) * 4;
+  if (smem > 48 * 1024 && ph::allow_dynamic_smem((const void*)k_tri_total<false, true>) != cudaSuccess) {
+    PH_CHECK_LAUNCH();
+    return PH_ERR_CUDA;
+  }
+  const int sms = ph::device_sms();
+  const int occ = ph::occupancy((const void*)k_tri_total<false, true>, SX_NT, smem);
+  const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
+  ph::count_launch();
+  ph::launch_pdl(k_tri_total<false, true>, dim3(grid), dim3(SX_NT), smem, s, adj_ptr, adj_idx, n, d_next,
+                 (unsigned long long*)nullptr, vcloud, want, d_per);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -590,7 +651,7 @@ extern "C" int ph_triangles_total_edges(const int32_t* edge_i, const int32_t* ed
   const int grid = (int)std::max<i64>(1, std::min<i64>(n, (i64)sms * std::max(occ, 1)));
   ph::count_launch();
   ph::launch_pdl(k_tri_total<true>, dim3(grid), dim3(SX_NT), smem, s, (const i32*)uptr, (const i32*)uidx, n, next,
-                 d_total);
+                 d_total, (const i32*)nullptr, (const uint8_t*)nullptr, (unsigned long long*)nullptr);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
@@ -602,7 +663,8 @@ extern "C" int ph_triangles_emit(const int32_t* edge_i, const int32_t* edge_j, i
   if (E <= 0) return E < 0 ? PH_ERR_ARG : PH_OK;
   ph::count_launch();
   ph::launch_pdl(k_triangles<true>, dim3(warp_grid(E)), dim3(SX_NT), 0, (cudaStream_t)stream, 
-      edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, nullptr, nullptr, tri_off, tri_m, tri_w, tri_fa, tri_fb);
+      edge_i, edge_j, E, adj_ptr, adj_idx, adj_rank, nullptr, nullptr, tri_off, tri_m, tri_w, tri_fa, tri_fb,
+      (const uint8_t*)nullptr, (const i32*)nullptr);
   PH_CHECK_LAUNCH();
   return PH_OK;
 }

@@ -232,6 +232,17 @@ size_t ph_triangles_total_edges_workspace_bytes(int64_t E, int64_t n);
 int ph_triangles_total_edges(const int32_t* edge_i, const int32_t* edge_j, int64_t E, int64_t n,
                              unsigned long long* d_total, void* workspace, size_t workspace_bytes, void* stream);
 
+/* ph_triangles_total per cloud of a batch's union graph (sorted rows of
+ * ph_vertex_csr over global vertices): vertex a's triangles go to
+ * d_per[vcloud[a]] (nclouds entries, zeroed here), and only the vertices of
+ * clouds with want[cloud] != 0 are visited. The batch form of the limit check
+ * of triangle_kernel.py:377-381: clouds that may be over max_triangles are
+ * counted exactly before the per-edge pass, which then skips those over it.
+ * n <= ph_triangles_total_max_vertices(); d_next: one int of device scratch. */
+int ph_batch_triangles_total(const int32_t* adj_ptr, const int32_t* adj_idx, int64_t n, const int32_t* vcloud,
+                             const uint8_t* want, int32_t nclouds, unsigned long long* d_per, int* d_next,
+                             void* stream);
+
 /* Writes, for every triangle in global order, its largest edge tri_m, third
  * vertex tri_w and the ranks of its two other edges (a,w) and (b,w): the emit
  * pass of triangle_kernel.py:288 triangle_enumerate with the face ranks of
