@@ -750,7 +750,7 @@ def kernel_breakdown(pts, t, max_dim, flush, reps=3):
 
 # DRAM traffic per launch from ncu captures of this workload (profiles/*.md)
 NCU_TRAFFIC = {
-    "k_tc_edges": {"bytes": 2.290e6 + 0.028e6, "source": "profiles/k_tc_edges_20k_d10.md"},
+    "k_tc_edges": {"bytes": 2.288e6, "source": "profiles/k_tc_edges_20k_d10.md"},
     "k_reduce": {"bytes": 0.8535e6, "source": "profiles/k_reduce_20k_d10_h1.md"},
     "k_cluster_sort": {"bytes": 0.389e6, "source": "profiles/k_cluster_sort_20k_d10.md"},
 }
