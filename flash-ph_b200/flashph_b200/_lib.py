@@ -73,6 +73,7 @@ _SIGS = {
     "ph_batch_result_free": (None, [P]),
     "ph_triangles_total_max_vertices": (I64, []),
     "ph_triangles_total": (ctypes.c_int, [P, P, I64, P, P, P]),
+    "ph_batch_triangles_total": (ctypes.c_int, [P, P, I64, P, P, I32, P, P, P]),
     "ph_edges_screened_workspace_bytes": (SZ, [I64, I32, I32]),
     "ph_batch_edges_enumerate_screened": (ctypes.c_int, [P, P, I32, I64, I32, I64, P, I64, P, P, P, I64, P, P, P,
                                                          P, SZ, P]),

@@ -84,6 +84,30 @@ def test_triangle_total_equals_per_edge_counts(n, d, t):
     assert int(tot.item()) == want
 
 
+@pytest.mark.parametrize("n,d,t", [(500, 3, 0.3), (1500, 10, 3.0), (3, 2, 9.0)])
+def test_batch_triangle_totals_per_cloud(n, d, t):
+    """ph_batch_triangles_total over a union of three copies of one graph
+    (vertices offset by n and 2n): each wanted cloud gets the single graph's
+    total, the cloud not wanted gets 0."""
+    from flashph_b200 import _lib as L
+    from flashph_b200.cohomology import count_triangles
+    from flashph_b200.rips import rips_filtration, vertex_csr
+    x = torch.from_numpy(np.random.default_rng(n + d).standard_normal((n, d)).astype(np.float32)).cuda()
+    f = rips_filtration(x, t)
+    E = f.edge_i.shape[0]
+    want_total = int(count_triangles(f)[E].item())
+    ei = torch.cat([f.edge_i + k * n for k in range(3)]).contiguous()
+    ej = torch.cat([f.edge_j + k * n for k in range(3)]).contiguous()
+    ptr, idx, _ = vertex_csr(ei, ej, 3 * n)
+    vcloud = torch.arange(3 * n, device="cuda", dtype=torch.int32) // n
+    want = torch.tensor([1, 0, 1], dtype=torch.uint8, device="cuda")
+    per = torch.full((3,), 7, dtype=torch.int64, device="cuda")
+    nxt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    L.call("ph_batch_triangles_total", ptr.data_ptr(), idx.data_ptr(), 3 * n, vcloud.data_ptr(), want.data_ptr(), 3,
+           per.data_ptr(), nxt.data_ptr(), L.stream_handle(x.device))
+    assert per.cpu().tolist() == [want_total, 0, want_total]
+
+
 def test_dense_call_over_the_triangle_limit_reports_the_exact_count():
     from flashph_b200 import rips_persistence
     pts = np.random.default_rng(5).standard_normal((3000, 3)).astype(np.float32)
