@@ -181,6 +181,37 @@ def _single_with_limits(p, t, md):
     return _compute_native(x, t, md, x.device, 2_000_000, 1_000_000)
 
 
+def test_exact_triangle_precount_under_and_over_the_limit():
+    """Clouds with more edges than the triangle bound allows for max_triangles
+    are counted exactly before the per-edge pass: one of them under the limit
+    (its diagrams must equal a single call's), one over it (the single call's
+    ValueError text, with the exact count), beside clouds too sparse to be
+    counted early."""
+    from flashph_b200.batch import rips_persistence_batch
+    from flashph_b200.persistence import _compute_native
+    rng = np.random.default_rng(41)
+    cap = 200_000  # the bound lets clouds of up to ~5.6K edges through uncounted
+    clouds = [rng.standard_normal((1000, 3)).astype(np.float32),          # counted early, under the limit
+              (rng.standard_normal((400, 3)) * 0.05).astype(np.float32),  # complete: C(400,3) over it
+              rng.standard_normal((300, 8)).astype(np.float32),
+              rng.standard_normal((64, 2)).astype(np.float32)]
+    ts = [0.6, 10.0, 2.2, 0.6]  # cloud 0: 9,305 edges and 40,242 triangles (oracle)
+    dims = [1, 1, 1, 1]
+    res = rips_persistence_batch(clouds, ts, dims, max_triangles=cap)
+    for c, (p, t, md, r) in enumerate(zip(clouds, ts, dims, res)):
+        x = torch.from_numpy(p).cuda()
+        try:
+            single = _compute_native(x, t, md, x.device, cap, 10_000_000)
+        except ValueError as ex:
+            assert isinstance(r, ValueError) and str(r) == str(ex), c
+            continue
+        assert not isinstance(r, Exception), (c, r)
+        for dim in range(md + 1):
+            assert _same(r[dim], single[dim]), (c, dim)
+    assert isinstance(res[1], ValueError) and "Triangle count 10586800 exceeds" in str(res[1])
+    assert not isinstance(res[0], Exception)
+
+
 def test_batch_split_by_the_simplex_budget(monkeypatch):
     """A budget small enough to split every chunk: the library reports the
     per-cloud counts, the batch is packed again, results are unchanged."""
