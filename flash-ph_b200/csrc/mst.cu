@@ -29,6 +29,9 @@ namespace ph {
 namespace {
 
 constexpr int MST_NT = 512;
+// forest mask value of an edge found inside one component: skipped by every
+// later round (components only merge), reset to 0 before the kernel ends
+constexpr uint8_t MST_DROPPED = 2;
 
 struct MstCtl {
   int last_offer_round;
@@ -85,11 +88,15 @@ __global__ void __launch_bounds__(MST_NT) k_mst(const i32* __restrict__ ei, cons
     // offers: the lowest-ranked edge leaving each root (no links in this phase)
     bool offered = false;
     for (i64 e = tid; e < E; e += nth) {
+      const uint8_t st = mst[e];
+      if (st == MST_DROPPED) continue;
       const i32 ru = find_root(parent, ei[e], status, ctl), rv = find_root(parent, ej[e], status, ctl);
       if (ru != rv) {
         if ((i32)e < *(volatile i32*)&best[ru]) atomicMin(&best[ru], (i32)e);
         if ((i32)e < *(volatile i32*)&best[rv]) atomicMin(&best[rv], (i32)e);
         offered = true;
+      } else if (st == 0) {
+        mst[e] = MST_DROPPED;  // inside one component for good: later rounds skip it
       }
     }
     if (__syncthreads_or(offered) && threadIdx.x == 0) ctl->last_offer_round = round;
@@ -121,6 +128,8 @@ __global__ void __launch_bounds__(MST_NT) k_mst(const i32* __restrict__ ei, cons
     }
     barrier(g);
   }
+  for (i64 e = tid; e < E; e += nth)
+    if (mst[e] == MST_DROPPED) mst[e] = 0;
   // labels: the root, which is the smallest vertex of its component
   long long roots = 0;
   for (i64 v = tid; v < n; v += nth) {
