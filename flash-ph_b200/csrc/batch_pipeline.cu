@@ -588,7 +588,13 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
   int64_t* t_off = A.take<int64_t>(K + 1);
   int64_t* row_off2 = A.take<int64_t>(K + 1);
   int64_t* nrows2 = A.take<int64_t>(1);
-  const size_t c2_b = ph_cofacet_csr_workspace_bytes(Q, 4), r2_b = ph_batch_persistence_rows_workspace_bytes(T);
+  // the H2 cofacet rows without a global sort when every row fits the per-row
+  // sorts: a triangle's tetrahedra number at most its cloud's points less 3
+  i64 max_n = 0;
+  for (int c = 0; c < K; ++c) max_n = std::max<i64>(max_n, segs[c].n);
+  const bool rows4 = max_n - 3 <= COF_ROWS_MAX;
+  const size_t c2_b = rows4 ? cofacet_rows_aos_workspace_bytes(T) : ph_cofacet_csr_workspace_bytes(Q, 4),
+               r2_b = ph_batch_persistence_rows_workspace_bytes(T);
   void* c2_ws = A.bytes(c2_b);
   void* r2_ws = A.bytes(r2_b);
   if (A.failed || cudaMallocAsync((void**)&res->rows[2], sizeof(float) * 2 * std::max<i64>(T, 1), s) != cudaSuccess)
@@ -603,7 +609,9 @@ extern "C" int ph_rips_persistence_batch(const float* const* points, const int64
     if (rc == PH_OK && T) rc = ph_or_gather_mask(skip2, en2, tri_m, T, 1, s);
     if (rc == PH_OK && Q) rc = ph_cof_max_face(tet_faces, nullptr, nullptr, nullptr, 4, Q, (i32)E, skip2, cmf2, s);
     if (rc == PH_OK && Q)
-      rc = ph_cofacet_csr(tet_faces, nullptr, nullptr, nullptr, 4, Q, T, (i32)(E + T), off2, data2, c2_ws, c2_b, s);
+      rc = rows4 ? cofacet_rows_aos(tet_faces, 4, Q, T, (i32)(E + T), off2, data2, st + 3, c2_ws, c2_b, s)
+                 : ph_cofacet_csr(tet_faces, nullptr, nullptr, nullptr, 4, Q, T, (i32)(E + T), off2, data2, c2_ws,
+                                  c2_b, s);
     if (rc != PH_OK) return give_up(rc);
     if (!Q) ph::zero_async(off2, sizeof(i32) * (T + 1), s);
     count_launch();

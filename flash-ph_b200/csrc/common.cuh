@@ -41,6 +41,11 @@ void count_launch();
 // The reducer's step cap per column (ph_set_reduce_limits; 2^24 by default)
 // and the cap on a native call's first reduction pool (0: none).
 long long reduce_max_steps();
+// the cofacet CSR of simplices given as k faces each, without a global sort (simplices.cu)
+constexpr int COF_ROWS_MAX = 8192;  // longest row the per-row sorts take
+size_t cofacet_rows_aos_workspace_bytes(int64_t n_faces);
+int cofacet_rows_aos(const int32_t* faos, int32_t k, int64_t S, int64_t n_faces, int32_t row_base, int32_t* cof_off,
+                     int32_t* cof_data, int* d_status, void* workspace, size_t workspace_bytes, cudaStream_t s);
 // the triangle count pass with an optional per-cloud mask (simplices.cu)
 int triangles_count_masked(const int32_t* edge_i, const int32_t* edge_j, int64_t E, const int32_t* adj_ptr,
                            const int32_t* adj_idx, const int32_t* adj_rank, int64_t* tri_off, int64_t* cof_off,

@@ -583,7 +583,10 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
   i32* cmf2 = A.take<i32>(Q);
   i32* off2 = A.take<i32>(T + 1);
   i32* data2 = A.take<i32>(4 * Q);
-  const size_t c2_b = ph_cofacet_csr_workspace_bytes(Q, 4);
+  // the H2 cofacet rows without a global sort when every row fits the per-row
+  // sorts: a triangle's tetrahedra number at most n - 3
+  const bool rows4 = n - 3 <= COF_ROWS_MAX;
+  const size_t c2_b = rows4 ? cofacet_rows_aos_workspace_bytes(T) : ph_cofacet_csr_workspace_bytes(Q, 4);
   void* c2_ws = A.bytes(c2_b);
   if (A.failed || cudaMallocAsync((void**)&res->rows[2], sizeof(float) * 2 * std::max<i64>(T, 1), s) != cudaSuccess)
     return alloc_fail();
@@ -595,7 +598,9 @@ extern "C" int ph_rips_persistence(const float* d_points, int64_t n, int32_t d, 
     if (rc == PH_OK) rc = ph_mark_pivots(r1.state, r1.piv, E, (i32)E, skip2, T, s);
     if (rc == PH_OK && Q) rc = ph_cof_max_face(tet_faces, nullptr, nullptr, nullptr, 4, Q, (i32)E, skip2, cmf2, s);
     if (rc == PH_OK && Q)
-      rc = ph_cofacet_csr(tet_faces, nullptr, nullptr, nullptr, 4, Q, T, (i32)(E + T), off2, data2, c2_ws, c2_b, s);
+      rc = rows4 ? cofacet_rows_aos(tet_faces, 4, Q, T, (i32)(E + T), off2, data2, st + 3, c2_ws, c2_b, s)
+                 : ph_cofacet_csr(tet_faces, nullptr, nullptr, nullptr, 4, Q, T, (i32)(E + T), off2, data2, c2_ws,
+                                  c2_b, s);
     if (rc != PH_OK) return give_up(rc);
     if (!Q) ph::zero_async(off2, sizeof(i32) * (T + 1), s);
   }

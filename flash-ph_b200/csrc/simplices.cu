@@ -383,6 +383,7 @@ __global__ void k_cmf(const i32* __restrict__ faos, const i32* __restrict__ f0, 
 // radix sort of all 3T entries by face, whose passes dominate dense batches.
 constexpr int RS_WARP_MAX = 1024;        // entries a warp sorts in shared memory
 constexpr int RS_BIG = 8192;             // entries a block sorts in shared memory
+static_assert(RS_BIG == ph::COF_ROWS_MAX, "the callers' row bound is the block sort's size");
 constexpr int RS_NT = 256;
 
 __global__ void k_off_i64_to_i32(const i64* __restrict__ in, i64 n, i32* __restrict__ out) {
@@ -408,6 +409,29 @@ __global__ void k_cof_scatter3(const i32* __restrict__ f0, const i32* __restrict
       if (pos < off[f[q] + 1]) data[pos] = r;
       else set_status(status, PH_ERR_ARG);
     }
+  }
+}
+
+// the cofacet rows of k-simplices given as k faces each (AoS): the row
+// lengths first (a count per face), then each simplex's rank into its faces'
+// rows; a write past its row's end is dropped and reported
+__global__ void k_cof_count_aos(const i32* __restrict__ faos, i64 H, i32* __restrict__ cnt) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < H; x += (i64)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[faos[x]], 1);
+}
+
+__global__ void k_cof_scatter_aos(const i32* __restrict__ faos, i64 H, int k, i32 row_base,
+                                  const i32* __restrict__ off, i32* __restrict__ cursor, i32* __restrict__ data,
+                                  int* status) {
+  ph::pdl_wait();
+  ph::pdl_trigger();
+  for (i64 x = (i64)blockIdx.x * blockDim.x + threadIdx.x; x < H; x += (i64)gridDim.x * blockDim.x) {
+    const i32 f = faos[x];
+    const i32 pos = off[f] + atomicAdd(&cursor[f], 1);
+    if (pos < off[f + 1]) data[pos] = row_base + (i32)(x / k);
+    else set_status(status, PH_ERR_ARG);
   }
 }
 
@@ -820,3 +844,58 @@ extern "C" int ph_cof_max_face(const int32_t* faces_aos, const int32_t* f0, cons
   PH_CHECK_LAUNCH();
   return PH_OK;
 }
+
+namespace ph {
+size_t cofacet_rows_aos_workspace_bytes(int64_t n_faces) {
+  const i64 nf = std::max<i64>(n_faces, 1);
+  return Carve::need(sizeof(i32) * (size_t)(nf + 1)) + 2 * Carve::need(sizeof(i32) * (size_t)nf) +
+         Carve::need(sizeof(int)) + Carve::need(scan_workspace_bytes(nf));
+}
+
+// The cofacet CSR of S simplices with k faces each (AoS, the tetrahedra's four
+// triangles) without a sort of the S k entries: rows counted, offsets scanned,
+// ranks scattered into their rows, each row sorted in shared memory. Rows must
+// hold at most RS_BIG entries (a triangle's tetrahedra number at most the
+// cloud's points less three: the caller checks that bound). The rows equal
+// ph_cofacet_csr's.
+int cofacet_rows_aos(const int32_t* faos, int32_t k, int64_t S, int64_t n_faces, int32_t row_base, int32_t* cof_off,
+                     int32_t* cof_data, int* d_status, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+  const i64 H = S * k;
+  if (k < 1 || S < 0 || n_faces < 0 || H >= (int64_t(1) << 31)) return PH_ERR_ARG;
+  Carve c(workspace, workspace_bytes);
+  const i64 nf = std::max<i64>(n_faces, 1);
+  i32* cnt = c.take<i32>(nf + 1);
+  i32* cursor = c.take<i32>(nf);
+  i32* big = c.take<i32>(nf);
+  int* nbig = c.take<int>(1);
+  void* sws = c.take<char>((i64)scan_workspace_bytes(nf));
+  if (!cnt || !cursor || !big || !nbig || !sws) return PH_ERR_ARG;
+  if (n_faces == 0) {
+    ph::zero_async(cof_off, sizeof(i32), s);
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  ph::zero_async(cnt, sizeof(i32) * (size_t)n_faces, s, cursor, sizeof(i32) * (size_t)n_faces);
+  ph::zero_async(nbig, sizeof(int), s);
+  if (H > 0) {
+    ph::count_launch();
+    ph::launch_pdl(k_cof_count_aos, dim3(grid_for(H)), dim3(256), 0, s, faos, H, cnt);
+  }
+  PH_TRY(scan_exclusive_i32_i32(cnt, cof_off, n_faces, sws, scan_workspace_bytes(nf), s));
+  if (H == 0) {
+    PH_CHECK_LAUNCH();
+    return PH_OK;
+  }
+  ph::count_launch();
+  ph::launch_pdl(k_cof_scatter_aos, dim3(grid_for(H)), dim3(256), 0, s, faos, H, (int)k, row_base,
+                 (const i32*)cof_off, cursor, cof_data, d_status);
+  const int gw = (int)std::max<i64>(1, std::min<i64>((n_faces + RS_NT / 32 - 1) / (RS_NT / 32), 148 * 16));
+  ph::count_launch();
+  ph::launch_pdl(k_cof_sort_rows, dim3(gw), dim3(RS_NT), 0, s, (const i32*)cof_off, n_faces, cof_data, big, nbig);
+  ph::count_launch();
+  ph::launch_pdl(k_cof_sort_big, dim3(148 * 2), dim3(RS_NT), 0, s, (const i32*)cof_off, cof_data, (const i32*)big,
+                 (const int*)nbig, d_status);
+  PH_CHECK_LAUNCH();
+  return PH_OK;
+}
+}  // namespace ph
